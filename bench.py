@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""PBD particle-steps/s on the 2,097,152-particle dam-break (one B200 per rank).
+
+One step = one dam-break frame through the C ABI (pk_pbf_step): box boundary,
+neighbour query (cap 64, radius 2.5 spacing), integration and 5 DensityPBD
+Jacobi iterations, on synthetic seeded inputs of the configuration's shape.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pk|reference]
+
+--impl reference times the CPU restatement of the same step (the reference is
+CUDA only; its kernel bodies restated in C with OpenMP) on the host cores, on
+a bounded sample of the workload per step.  With N > 1 (torchrun) the scene
+does not shard: every rank steps its own replica ("replicas only").
+"""
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "physika-old_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+import scenes  # noqa: E402
+
+METRIC = "PBD particle-steps/s at 2M (HBM %roofline); batched+adjoint vs plain, same GPU"
+UNIT = "particle-steps/s"
+
+
+def pbd_bytes_per_particle_step(kbar, iters):
+    """Algorithmic HBM bytes of one PBD particle-step: neighbour build (read x,
+    write list + count), integration, per iteration pass A (x, list, lambda) and
+    pass B (x, lambda, list, x'), velocity update, density out, boundary pass."""
+    return 176.0 + 4.0 * kbar + iters * (44.0 + 8.0 * kbar)
+
+
+def pass_bytes(kind, kbar, kunion):
+    """Algorithmic bytes per particle of one launch of a solver pass."""
+    if kind == "density":  # read x_i, the N(i) row, write lambda
+        return 12.0 + 4.0 * kbar + 4.0
+    if kind == "disp":  # read x_i, lambda_i, the row, write x_i'
+        return 12.0 + 4.0 + 4.0 * kunion + 12.0
+    raise ValueError(kind)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.bus_id = (bus_id or "").lower()
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [s.strip() for s in line.split(",")]
+            if len(f) < 10:
+                continue
+            if self.bus_id and self.bus_id not in f[1].lower():
+                continue
+            rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
+        out.update(sm_mhz=statistics.median(sm) if sm else None,
+                   sm_max_mhz=float(rows[0][3]) if rows[0][3].replace(".", "").isdigit() else None,
+                   reasons=reasons, samples=len(rows))
+        return out
+
+
+def bus_id_of(dev):
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(dev)
+        return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}"
+    except Exception:
+        return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# --------------------------------------------------------------- CPU arm
+
+def cpu_step_sample(sc_params, x, v, sdf, rnd):
+    import pk_oracle as po
+    x, v = po.sdf_constrain(x, v, sdf, rnd, 0.95, 0.0, sc_params.dt)
+    ri, re = po.neighbor_query(x, sc_params.radius, sc_params.lo, sc_params.hi, sc_params.cap)
+    x, v = po.integrate(x, v, sc_params.gravity, sc_params.dt)
+    f, m = po.density_scaling(sc_params.spacing, sc_params.radius, sc_params.rest_density)
+    x, v, _ = po.pbd_constrain(x, v, ri, re, sc_params.cap, sc_params.radius, f * m,
+                               sc_params.iterations, sc_params.dt)
+    return x, v
+
+
+def cpu_sample_scene():
+    # 64^3 = 262,144 particles with the 2M scene's spacing, radius, cap, dt
+    return scenes.dam_break_2m(seed=0, n_side=64)
+
+
+def time_cpu(steps, warmup, threads=0):
+    import pk_oracle as po
+    po.set_threads(threads)
+    sc = cpu_sample_scene()
+    sdf = po.sdf_box(sc.lo, sc.hi, sc.sdf_spacing, True)
+    rnd = np.random.default_rng(0).uniform(0, 1, sc.x.shape[0]).astype(np.float32)
+    x, v = sc.x.copy(), sc.v.copy()
+    for _ in range(warmup):
+        x, v = cpu_step_sample(sc, x, v, sdf, rnd)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        x, v = cpu_step_sample(sc, x, v, sdf, rnd)
+    dt = time.perf_counter() - t0
+    return sc.x.shape[0] * steps / dt, po.max_threads(), sc.x.shape[0]
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    v, cores, n = time_cpu(args.steps, args.warmup)
+    sample = (f"{n} particles (64^3 block, 2M-scene spacing/radius/cap 64/dt/5 iterations) "
+              f"per step, CPU restatement with OpenMP")
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": n / v * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "dam_break_2m sample", "particles": n, "cap": 64, "iterations": 5},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU arm
+
+def load_traffic():
+    """ncu DRAM bytes per launch of the dominant kernel, from the committed
+    profile summary (None when no capture has been summarised yet)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
+def run_pk(args):
+    import torch
+    import torch.distributed as dist
+    import pkhot
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    sc = scenes.dam_break_2m(seed=0)
+    n = sc.x.shape[0]
+    ctx = pkhot.Context(local)
+    ctx.boundary_set_box(sc.lo, sc.hi, sc.sdf_spacing, True)
+    x = torch.from_numpy(sc.x.copy()).to(dev)
+    v = torch.from_numpy(sc.v.copy()).to(dev)
+    prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
+                           pkhot.pbd_params(sc.radius, sc.spacing, sc.rest_density, sc.iterations, sc.dt),
+                           sc.gravity, boundary=True)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(val):
+        if world == 1:
+            return val
+        t = torch.tensor([val], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # K-bar (list counts incl. self) and the solver-row length of the start state
+    ctx.nq_build(x, sc.radius, sc.lo, sc.hi, sc.cap, want_list=False)
+    kbar, kunion, kmax = ctx.row_stats()
+
+    for _ in range(args.warmup):
+        ctx.pbf_step(x, v, prm)
+    ctx.check_status()
+    launches_per_step = ctx.launch_count()
+    barrier()
+
+    clocks = Clocks(bus_id_of(local))
+    clocks.start()
+    ctx.profile(True)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.pbf_step(x, v, prm)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    clk = clocks.stop()
+    ctx.check_status()
+    ms_max = max_over_ranks(ms)
+    value = world * n * args.steps / (ms_max / 1e3)
+
+    # ---- end to end through the public call with host buffers
+    e2e_steps = max(3, min(args.steps, 20))
+    xh = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    vh = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    xh.copy_(x.cpu())
+    vh.copy_(v.cpu())
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        x.copy_(xh, non_blocking=True)
+        v.copy_(vh, non_blocking=True)
+        ctx.pbf_step(x, v, prm)
+        xh.copy_(x, non_blocking=True)
+        vh.copy_(v, non_blocking=True)
+    f1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    e2e_val = world * n * e2e_steps / (e2e_ms / 1e3)
+    ctx.check_status()
+
+    peak, peak_kind = peaks()
+    # dominant kernel class over the timed region
+    dom = max(("density", "disp"), key=lambda k: prof[k][0])
+    dom_ms, dom_launches = prof[dom]
+    traffic = load_traffic().get(dom)
+    # rows of the displacement pass hold N(i) plus the mirror entries (kunion)
+    per_launch_bytes = n * pass_bytes(dom, kbar, kunion)
+    achieved = per_launch_bytes / (dom_ms / dom_launches / 1e3) / 1e9
+    step_bytes = pbd_bytes_per_particle_step(kbar, sc.iterations)
+    step_frac = value / world * step_bytes / (peak * 1e9)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "dam_break_2m: 128^3 jittered lattice, spacing 0.0025, radius 0.00625, "
+                               "cap 64, 5 Jacobi iterations, dt 5e-4, box 2x1x1",
+                   "particles": n, "kbar": kbar, "solver_row_mean": kunion,
+                   "solver_row_max": kmax, "iterations": sc.iterations,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set > L2 (neighbour rows alone are > 1 GB); no flush"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes},
+        "step_roofline": {"bytes_per_particle_step": step_bytes, "frac": step_frac,
+                          "peak_source": peak_kind},
+        "kernel_ms": {k: {"total_ms": prof[k][0], "launches": prof[k][1]} for k in prof},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+                "d2h_bytes_per_step": 2 * n * 12, "steps": e2e_steps},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cv, cores, cn = time_cpu(steps=2, warmup=1)
+        line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"2 steps of a {cn}-particle block with the 2M scene's "
+                                          "parameters, CPU restatement, OpenMP"}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="pk", choices=["pk", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_pk(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

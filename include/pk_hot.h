@@ -1,0 +1,223 @@
+/*
+ * pk_hot.h -- C ABI of the B200-native particle-constraint hot path.
+ *
+ * One shared library (physika-old_b200/lib/libpkhot.so) exports these
+ * symbols.  Arguments are plain device pointers and sizes; no C++ or torch
+ * types cross the boundary.  Every entry point returns an int status
+ * (PK_OK = 0) and never frees caller memory.  Positions, velocities and
+ * forces are the reference's DeviceArray<Vector3f>: 3 floats per particle,
+ * 12-byte stride, in the caller's particle order.  Neighbour lists use the
+ * reference's NeighborList<int> layouts (Framework/Topology/NeighborList.h:27-66):
+ *   cap > 0  (fixed):   index[i] = count_i, elements[i*cap + k]
+ *   cap == 0 (dynamic): index[i] = exclusive CSR offset, elements packed
+ *
+ * All work is enqueued on `stream` (NULL = legacy default stream) without a
+ * host synchronisation, except where a function says it synchronises.
+ * Conditions found on the device (a row over capacity) are latched in the
+ * context and reported by pk_ctx_status().
+ *
+ * Reference paths below are relative to PhysIKA's source tree (Source/).
+ */
+#ifndef PK_HOT_H
+#define PK_HOT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pk_ctx pk_ctx;
+typedef struct CUstream_st* pk_stream; /* a cudaStream_t */
+
+enum {
+    PK_OK = 0,
+    PK_ERR_ARG = 1,      /* invalid argument (null pointer, negative size, ...) */
+    PK_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+    PK_ERR_CAPACITY = 3, /* a list or buffer capacity was exceeded */
+    PK_ERR_STATE = 4,    /* call order violated (e.g. solve before init) */
+    PK_ERR_NOMEM = 5     /* device allocation failed */
+};
+
+/* ------------------------------------------------------------- context */
+
+/* Creates a context on `device`.  The context owns the module scratch (the
+ * role of DensityPBD::m_lamda/m_deltaPos, GridHash::ids/counter/index,
+ * ElasticityModule::m_invK/m_weights ...: DensityPBD.h:82-84,
+ * GridHash.h:90-92, ElasticityModule.h:96-106).  Scratch grows on demand and
+ * is kept, so steady-state steps allocate nothing. */
+int pk_ctx_create(pk_ctx** out, int device);
+int pk_ctx_destroy(pk_ctx* ctx);
+/* Message of the last failing call on this context ("" if none). */
+const char* pk_last_error(const pk_ctx* ctx);
+/* Synchronises `stream`, returns and clears conditions latched on the device:
+ * PK_ERR_CAPACITY if a neighbour row or list overflowed since the last call. */
+int pk_ctx_status(pk_ctx* ctx, pk_stream stream);
+
+/* ------------------------------------------------------ NeighborQuery */
+
+typedef struct {
+    float radius;      /* NeighborQuery::inRadius (NeighborQuery.h:57) */
+    float lo[3];       /* scene bounds (NeighborQuery::setBoundingBox, NeighborQuery.h:30) */
+    float hi[3];
+    int cap;           /* setNeighborSizeLimit (NeighborQuery.h:34); 0 = dynamic list */
+    int max_neighbors; /* dynamic mode only: per-particle row bound (0 = 256) */
+} pk_nq_params;
+
+/* NeighborQuery::compute (Framework/Topology/NeighborQuery.cu:152-199):
+ * GridHash::construct (GridHash.cu:297-323) then queryNeighborFixed
+ * (NeighborQuery.cu:584-605) or queryNeighborDynamic (:450-478).  Fixed mode
+ * keeps the `cap` nearest; the set equals the reference's replace-the-farthest
+ * result (exactly equal distances at the cap boundary are ordered
+ * deterministically here, by arrival order in the reference).
+ *
+ * `x` is read (n AoS positions).  index/elements may be NULL (only the
+ * context's internal list is built, which pk_pbd_solve/pk_pbf_step use).
+ * Fixed mode writes index[n] and elements[n*cap] (elements_capacity >= n*cap).
+ * Dynamic mode writes CSR offsets to index[n] and, if the total fits,
+ * elements; when `total` is non-NULL this call synchronises `stream` and
+ * stores the number of entries (and returns PK_ERR_CAPACITY if it exceeded
+ * elements_capacity, as the reference re-sizes its list, NeighborQuery.cu:463-472). */
+int pk_nq_build(pk_ctx* ctx, const float* x, int n, const pk_nq_params* p,
+                int* index, int* elements, long long elements_capacity,
+                long long* total, pk_stream stream);
+
+/* Row statistics of the context's last neighbour build (synchronises
+ * `stream`): mean entries of N(i) (the capped list incl. self), mean entries
+ * of the solver rows (N(i) plus the particles whose capped list holds i) and
+ * the longest solver row.  No reference counterpart (measurement only). */
+int pk_nq_row_stats(pk_ctx* ctx, double* mean_list, double* mean_row, int* max_row,
+                    pk_stream stream);
+
+/* ---------------------------------------------------------- DensityPBD */
+
+typedef struct {
+    float smoothing_length;  /* varSmoothingLength (DensityPBD.h:44) */
+    float sampling_distance; /* varSamplingDistance (DensityPBD.h:42) */
+    float rest_density;      /* varRestDensity (DensityPBD.h:40); only sets mass */
+    int iterations;          /* varIterationNumber (DensityPBD.h:38) */
+    float dt;                /* parent Node's dt (DensityPBD.cu:308) */
+} pk_pbd_params;
+
+/* SummationDensity::compute (Dynamics/ParticleSystem/SummationDensity.cu:58-110,
+ * K_ComputeDensity :13-36) over any NeighborList<int>.  rho[n] written. */
+int pk_summation_density(pk_ctx* ctx, const float* x, int n, const int* index,
+                         const int* elements, int cap, long long total,
+                         const pk_pbd_params* p, float* rho, pk_stream stream);
+
+/* DensityPBD::constrain (Dynamics/ParticleSystem/DensityPBD.cu:271-302):
+ * `iterations` Jacobi sweeps of density, lambda (K_ComputeLambdas :46-90) and
+ * displacement (K_ComputeDisplacement :134-179, K_UpdatePosition :226-237),
+ * then v += (x - x_old)/dt (DP_UpdateVelocity :367-378).  x and v are updated
+ * in place; rho_out (may be NULL) receives outDensity.  When (index, elements)
+ * are the arrays the last pk_nq_build on this context wrote (and n matches),
+ * the solve runs on the context's sorted internal list; any other list is
+ * solved as given. */
+int pk_pbd_solve(pk_ctx* ctx, float* x, float* v, int n, const int* index,
+                 const int* elements, int cap, long long total,
+                 const pk_pbd_params* p, float* rho_out, pk_stream stream);
+
+/* ---------------------------------------------------- ParticleIntegrator */
+
+/* ParticleIntegrator::integrate (Dynamics/ParticleSystem/ParticleIntegrator.cu:128-138):
+ * v += dt*(f + g) (K_UpdateVelocity :59-70), then x += dt*v (K_UpdatePosition
+ * :102-112).  f may be NULL (ParticleIntegrator::begin zeroes it, :32). */
+int pk_integrate(pk_ctx* ctx, float* x, float* v, const float* f, int n,
+                 const float gravity[3], float dt, pk_stream stream);
+
+/* ------------------------------------------------- BoundaryConstraint */
+
+/* BoundaryConstraint::setCube (Dynamics/ParticleSystem/BoundaryConstraint.cu:108-117):
+ * a box SDF on a grid of `spacing` with 5 cells of padding
+ * (DistanceField3D::setSpace/loadBox, Framework/Topology/DistanceField3D.cu:194-201,266-291).
+ * inverted != 0 keeps particles inside the box.  Replaces the context's box. */
+int pk_boundary_set_box(pk_ctx* ctx, const float lo[3], const float hi[3], float spacing,
+                        int inverted, pk_stream stream);
+
+/* BoundaryConstraint::constrain (BoundaryConstraint.cu:84-97, K_ConstrainSDF
+ * :29-67): particles with SDF distance <= 0 are projected out along the SDF
+ * normal plus 1e-4*U with U = curand_uniform after curand_init(particle id,0,0),
+ * their normal velocity is reflected and scaled by (1 - normal_friction). */
+int pk_boundary_constrain(pk_ctx* ctx, float* x, float* v, int n, float normal_friction,
+                          float tangential_friction, float dt, pk_stream stream);
+
+/* The jitter values K_ConstrainSDF draws (BoundaryConstraint.cu:50-51):
+ * out[i] = curand_uniform after curand_init(i, 0, 0) (RandNumber,
+ * Core/Utility/CudaRand.h:12-24), for i < n. */
+int pk_boundary_jitter(pk_ctx* ctx, int n, float* out, pk_stream stream);
+
+/* ---------------------------------------------- fused fluid step */
+
+typedef struct {
+    pk_nq_params nq;       /* neighbour query of the step */
+    pk_pbd_params pbd;     /* DensityPBD parameters (pbd.dt is the step's dt) */
+    float gravity[3];      /* SceneGraph::getGravity (Framework/Framework/SceneGraph.h:57-58) */
+    int boundary;          /* 1: apply the context's box boundary first */
+    float normal_friction; /* BoundaryConstraint.h:32 default 0.95 */
+    float tangential_friction;
+} pk_pbf_params;
+
+/* One dam-break frame: StaticBoundary::advance (StaticBoundary.cpp:45-59) then
+ * PositionBasedFluidModel::step without viscosity
+ * (Dynamics/ParticleSystem/PositionBasedFluidModel.cpp:83-101): integrator
+ * begin, NeighborQuery on the current positions, integrate, DensityPBD.
+ * x, v (n AoS) are updated in place; rho_out may be NULL.  Asynchronous and
+ * allocation-free once the context has seen `n` (capturable in a CUDA graph). */
+int pk_pbf_step(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p,
+                float* rho_out, pk_stream stream);
+
+/* Number of kernel launches the last pk_pbf_step enqueued. */
+int pk_last_launch_count(const pk_ctx* ctx);
+
+/* Per-kernel timing with CUDA events recorded on the launching stream around
+ * each kernel class of the neighbour build and the solver (no reference
+ * counterpart; the reference's GTimer, Core/Utility/GTimer.h:6-23, is the
+ * closest).  pk_ctx_profile(ctx, 1) clears and starts recording;
+ * pk_ctx_profile_read synchronises and returns the summed milliseconds and
+ * launch count of one class:
+ *   0 sort (keys, cell scan, scatter, cell fix-up, gather), 1 cap selection,
+ *   2 row emission, 3 density+lambda pass, 4 displacement pass, 5 write-back. */
+enum { PK_PROF_SORT = 0, PK_PROF_SELECT, PK_PROF_EMIT, PK_PROF_DENSITY, PK_PROF_DISP,
+       PK_PROF_FINISH, PK_PROF_KINDS };
+int pk_ctx_profile(pk_ctx* ctx, int enable);
+int pk_ctx_profile_read(pk_ctx* ctx, int kind, double* total_ms, int* launches);
+
+/* ---------------------------------------------- ElasticityModule (peridynamics) */
+
+typedef struct {
+    float horizon;   /* inHorizon (ElasticityModule.h:63) */
+    float mu;        /* m_mu, default 0.05 (ElasticityModule.cu:326) */
+    float lambda;    /* m_lambda, default 0.1 (ElasticityModule.cu:327) */
+    int iterations;  /* m_iterNum, default 10 (ElasticityModule.cu:328) */
+    float dt;
+    float break_stretch; /* > 0: bonds break when |x_i-x_j| > (1+s)|r_ij| (no reference counterpart) */
+} pk_pd_params;
+
+/* ElasticityModule::initializeImpl (Dynamics/ParticleSystem/ElasticityModule.cu:519-546):
+ * freezes the rest shape from the neighbour list (resetRestShape +
+ * K_UpdateRestShape :449-517, self moved to slot 0), sets bulk stiffness 1
+ * (computeMaterialStiffness :380-387) and precomputes K^-1 once
+ * (EM_PrecomputeShape :21-116; the rest shape never changes, so the
+ * reference's per-step recomputation gives the same matrix). */
+int pk_pd_init(pk_ctx* ctx, const float* x, int n, const int* index, const int* elements,
+               int cap, long long total, float horizon, pk_stream stream);
+
+/* The protected ElasticityModule::m_bulkCoefs (ElasticityModule.h:96) that
+ * subclasses set through computeMaterialStiffness: bulk[n] is copied. */
+int pk_pd_set_bulk(pk_ctx* ctx, const float* bulk, int n, pk_stream stream);
+
+/* ElasticityModule::solveElasticity (ElasticityModule.cu:404-421): iterations
+ * of EM_EnforceElasticity (:123-242) + K_UpdatePosition (:281-292), then
+ * K_UpdateVelocity (:295-306).  x, v in place (n AoS). */
+int pk_pd_solve(pk_ctx* ctx, float* x, float* v, int n, const pk_pd_params* p,
+                pk_stream stream);
+
+/* Copies the frozen rest shape out: rest_idx/rest_pos in the NeighborList
+ * layout the rest shape was built with (TPair index/pos, Dynamics/ParticleSystem/NeighborData.h:6-21). */
+int pk_pd_get_rest_shape(pk_ctx* ctx, int* rest_idx, float* rest_pos, float* inv_k,
+                         pk_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

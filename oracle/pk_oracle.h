@@ -1,0 +1,112 @@
+/*
+ * pk_oracle.h -- CPU restatement of PhysIKA's particle-constraint hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the CUDA library, the
+ * C++ Framework mirror, the Python wrapper) may call, link or load this code.
+ * It is used by tests/ as the checker, by __graft_entry__.smoke() to check one
+ * small GPU invocation, and by bench.py as the timed CPU baseline
+ * (cpu_baseline / --impl reference).
+ *
+ * Every function restates one reference kernel or host routine and cites the
+ * reference file:line it follows (paths relative to the PhysIKA source tree).
+ *
+ * Precision: the neighbour query, grid and SDF are float only (the reference
+ * computes them in float).  The solver functions exist in two builds of the
+ * same source: suffix _f (float, the reference's precision) and _d (double,
+ * the FP64 oracle of the same method, used for error statements only).
+ *
+ * Layout: positions/velocities/forces are AoS arrays of 3 values per particle
+ * (Vector3f, 12 B stride), exactly as the reference's DeviceArray<Coord>.
+ * Neighbour lists use NeighborList<int>'s two layouts (NeighborList.h:27-66):
+ *   cap > 0 : index[i] = count_i, elements[i*cap + k]
+ *   cap == 0: index[i] = exclusive CSR offset, elements packed, `total` entries
+ */
+#ifndef PK_ORACLE_H
+#define PK_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* GridHash geometry (GridHash.cu:46-75). */
+typedef struct {
+    float ds;        /* cell size = radius */
+    float lo[3];     /* padded lower corner */
+    int nx, ny, nz;  /* cells per axis */
+} pko_grid;
+
+void  pko_grid_setup(pko_grid* g, float h, const float lo[3], const float hi[3]);
+/* Which float expression computes |a-b|.  0: ((x*x+y*y)+z*z), 1:
+ * fma(z,z,fma(x,x,y*y)), 2: fma(z,z,fma(y,y,x*x)).  Must equal the variant the
+ * CUDA library was built with for neighbour sets to be bit-exact. */
+void  pko_set_norm_variant(int v);
+int   pko_get_norm_variant(void);
+float pko_dist3(const float* a, const float* b);
+
+/* NeighborQuery::compute (NeighborQuery.cu:152-199) with GridHash::construct
+ * (GridHash.cu:297-323).  Fixed mode (cap > 0) follows K_ComputeNeighborFixed
+ * (NeighborQuery.cu:514-581); dynamic mode (cap == 0) follows K_CalNeighborSize
+ * + scan + K_GetNeighborElements (NeighborQuery.cu:245-276,337-367,450-478).
+ * Particles in one cell are visited in ascending id (the reference's order is
+ * whatever its atomics produced).  In dynamic mode, pass elements == NULL to
+ * obtain *total only.  Returns 0, or -1 if elem_capacity is too small. */
+int pko_neighbor_query(int n, const float* x, float h, const float lo[3], const float hi[3],
+                       int cap, int* index, int* elements, long long elem_capacity,
+                       long long* total);
+
+/* SummationDensity::calculateScalingFactor (SummationDensity.cu:112-138):
+ * factor = 1/sum(V*W) over a lattice, mass = rho0*d^3; the kernels then use
+ * factor*mass (SummationDensity.cu:104-109). */
+void pko_density_scaling(float sampling, float h, float rho0, float* factor, float* mass);
+
+/* Box SDF on a grid: BoundaryConstraint::setCube (BoundaryConstraint.cu:108-117)
+ * -> DistanceField3D::setSpace (DistanceField3D.cu:194-201) + loadBox
+ * (DistanceField3D.cu:266-291).  `data` must hold (nx+11)*(ny+11)*(nz+11)
+ * floats, nx = floor((hi-lo)/spacing); pass data == NULL to get the dims. */
+typedef struct {
+    float left[3];   /* m_left */
+    float h[3];      /* m_h (cell size per axis) */
+    int   nx, ny, nz;/* node counts (m_distance dims) */
+    int   inverted;
+    float* data;     /* nx*ny*nz node values, x fastest */
+} pko_sdf;
+void pko_sdf_box_dims(const float lo[3], const float hi[3], float spacing, int dims[3]);
+void pko_sdf_box_fill(pko_sdf* s, const float lo[3], const float hi[3], float spacing, int inverted);
+
+/* DistanceField3D::getDistance (DistanceField3D.h:113-170). */
+void pko_sdf_distance(const pko_sdf* s, const float p[3], float* d, float normal[3]);
+
+/* K_ConstrainSDF (BoundaryConstraint.cu:29-67).  rnd[i] is the value
+ * curand_uniform returns after curand_init(i, 0, 0) (CudaRand.h:12-24); the
+ * generator is not restated: the table is produced by curand on a GPU. */
+void pko_sdf_constrain(int n, float* x, float* v, const pko_sdf* s, const float* rnd,
+                       float normal_friction, float tangential_friction, float dt);
+
+/* ---- solver, float (_f) and double (_d) builds of the same source ---- */
+#define PKO_DECLARE(real, sfx)                                                               \
+void pko_summation_density##sfx(int n, const real* x, const int* index, const int* elements, \
+                                int cap, long long total, real h, real mass, real* rho);     \
+void pko_pbd_constrain##sfx(int n, real* x, real* v, const int* index, const int* elements,  \
+                            int cap, long long total, real h, real mass, int iterations,     \
+                            real dt, real* rho_out);                                         \
+void pko_integrate##sfx(int n, real* x, real* v, const real* f, const real g[3], real dt);  \
+void pko_pd_rest_shape##sfx(int n, const real* x, const int* index, const int* elements,     \
+                            int cap, long long total, int* rest_idx, real* rest_pos);        \
+void pko_pd_inverse_k##sfx(int n, const int* index, int cap, long long total,                \
+                           const real* rest_pos, real h, real* invK);                        \
+void pko_pd_solve##sfx(int n, real* x, real* v, const int* index, int cap, long long total,  \
+                       const int* rest_idx, const real* rest_pos, const unsigned char* alive,\
+                       const real* invK, const real* bulk, real horizon, real mu,            \
+                       real lambda, int iterations, real dt);
+
+PKO_DECLARE(float, _f)
+PKO_DECLARE(double, _d)
+
+/* Threads used by the OpenMP loops (0 = library default). 1 = deterministic. */
+void pko_set_threads(int t);
+int  pko_max_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,46 @@
+"""Builds libpkhot.so (sm_100a) in-tree.  Incremental: skips when up to date."""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CU_SOURCES = ["pk_sort.cu", "pk_nbr.cu", "pk_pbd.cu", "pk_pd.cu", "pk_api.cu"]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_pkhot(force=False, verbose=True):
+    out = os.path.join(HERE, "lib", "libpkhot.so")
+    srcs = [os.path.join(HERE, "csrc", s) for s in CU_SOURCES]
+    deps = srcs + glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + [
+        os.path.join(ROOT, "include", "pk_hot.h")]
+    if not force and not _newer(out, deps):
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17",
+           "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
+           "-shared", "-o", out + ".tmp", *srcs]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build_oracle(verbose=True):
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True,
+                   stdout=None if verbose else subprocess.DEVNULL)
+
+
+if __name__ == "__main__":
+    build_pkhot(force="--force" in sys.argv)
+    build_oracle()

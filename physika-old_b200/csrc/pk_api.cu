@@ -1,0 +1,724 @@
+// pk_api.cu -- the extern "C" entry points declared in include/pk_hot.h.
+//
+// Validation happens here, on the host, before anything is enqueued; the
+// kernels assume valid sizes.  Scratch grows on demand (cudaMalloc outside
+// any capture; once a size has been seen nothing is allocated again).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "pk_kernels.cuh"
+
+#define PK_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+int fail(pk_ctx* c, int code, const char* msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(pk_ctx* c, cudaError_t e, const char* where)
+{
+    if (c) {
+        c->err = std::string(where) + ": " + cudaGetErrorString(e);
+    }
+    return PK_ERR_CUDA;
+}
+
+// Launch errors of everything enqueued since the last check.
+int check_launch(pk_ctx* c, const char* where)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, where);
+    return PK_OK;
+}
+
+template <class T>
+bool regrow(T*& p, size_t count)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)&p, sizeof(T) * count) == cudaSuccess;
+}
+
+int ensure_particles(pk_ctx* c, int n)
+{
+    if (n <= c->cap_n) return PK_OK;
+    size_t m = (size_t)n;
+    bool ok = regrow(c->perm, m) && regrow(c->inv, m) && regrow(c->key, m) && regrow(c->rank, m) &&
+              regrow(c->count, m) && regrow(c->count_c, m) && regrow(c->offs, m + 1) &&
+              regrow(c->xs_pre, m) && regrow(c->xs0, m) && regrow(c->xa, m) && regrow(c->xb, m) &&
+              regrow(c->vs, m) && regrow(c->lam, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
+              regrow(c->tau, m);
+    if (!ok) {
+        c->cap_n = 0;
+        return fail(c, PK_ERR_NOMEM, "device allocation of particle scratch failed");
+    }
+    c->cap_n = n;
+    return PK_OK;
+}
+
+int ensure_rows(pk_ctx* c, long long m)
+{
+    if (m <= c->cap_rows) return PK_OK;
+    if (!regrow(c->rows, (size_t)m)) {
+        c->cap_rows = 0;
+        return fail(c, PK_ERR_NOMEM, "device allocation of neighbour rows failed");
+    }
+    c->cap_rows = m;
+    return PK_OK;
+}
+
+int ensure_keys(pk_ctx* c, long long nk, int n)
+{
+    if (nk > c->cap_keys) {
+        if (!regrow(c->cell_cnt, (size_t)nk + 1) || !regrow(c->cell_start, (size_t)nk + 2)) {
+            c->cap_keys = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of the cell table failed");
+        }
+        c->cap_keys = nk;
+    }
+    long long parts = std::max(pk::scan_parts_needed(nk + 1), pk::scan_parts_needed(n));
+    if (parts > c->cap_part) {
+        if (!regrow(c->scan_part, (size_t)parts)) {
+            c->cap_part = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of scan partials failed");
+        }
+        c->cap_part = parts;
+    }
+    return PK_OK;
+}
+
+int ensure_generic(pk_ctx* c, int n)
+{
+    if (n <= c->cap_g) return PK_OK;
+    size_t m = (size_t)n;
+    if (!(regrow(c->g_rho, m) && regrow(c->g_lam, m) && regrow(c->g_dpos, 3 * m) &&
+          regrow(c->g_xold, 3 * m))) {
+        c->cap_g = 0;
+        return fail(c, PK_ERR_NOMEM, "device allocation of solver scratch failed");
+    }
+    c->cap_g = n;
+    return PK_OK;
+}
+
+int row_capacity(const pk_nq_params* p)
+{
+    if (p->cap > 0) return ((p->cap + 64 + 31) / 32) * 32;
+    int m = p->max_neighbors > 0 ? p->max_neighbors : 256;
+    return std::min(m, pk::kMaxHits);
+}
+
+int check_nq(pk_ctx* c, const pk_nq_params* p)
+{
+    if (!p) return fail(c, PK_ERR_ARG, "null neighbour-query parameters");
+    if (!(p->radius > 0.0f) || !std::isfinite(p->radius))
+        return fail(c, PK_ERR_ARG, "radius must be positive and finite");
+    if (p->cap < 0 || p->cap > 448) return fail(c, PK_ERR_ARG, "cap must be in [0, 448]");
+    if (p->max_neighbors < 0 || p->max_neighbors > pk::kMaxHits)
+        return fail(c, PK_ERR_ARG, "max_neighbors must be in [0, 512]");
+    for (int a = 0; a < 3; ++a)
+        if (!(p->hi[a] > p->lo[a])) return fail(c, PK_ERR_ARG, "bounding box must have hi > lo");
+    pk::Grid g = pk::make_grid(p->radius, p->lo, p->hi);
+    if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || g.nkeys > (1LL << 30))
+        return fail(c, PK_ERR_ARG, "grid too large for the radius and bounds");
+    return PK_OK;
+}
+
+// SummationDensity::calculateScalingFactor (SummationDensity.cu:112-138) in
+// host float arithmetic; returns factor * mass, the mass the kernels use.
+float effective_mass(const pk_pbd_params* p)
+{
+    const float d = p->sampling_distance, H = p->smoothing_length;
+    const float V = d * d * d;
+    float total = 0.0f;
+    const int half = (int)(H / d + 1.0f);
+    for (int i = -half; i <= half; ++i)
+        for (int j = -half; j <= half; ++j)
+            for (int k = -half; k <= half; ++k) {
+                float x = (float)i * d, y = (float)j * d, z = (float)k * d;
+                float r = std::sqrt(x * x + y * y + z * z);
+                float q = r / H, w = 0.0f;
+                if (!(q > 1.0f)) {
+                    float dd = (float)(1.0 - (double)q);
+                    float hh = H * H;
+                    w = 15.0f / ((float)M_PI * hh * H) * dd * dd * dd;
+                }
+                total += V * w;
+            }
+    const float factor = (float)(1.0 / (double)total);
+    return factor * (p->rest_density * V);
+}
+
+int check_pbd(pk_ctx* c, const pk_pbd_params* p)
+{
+    if (!p) return fail(c, PK_ERR_ARG, "null DensityPBD parameters");
+    if (!(p->smoothing_length > 0.0f) || !(p->sampling_distance > 0.0f) || !(p->dt > 0.0f))
+        return fail(c, PK_ERR_ARG, "smoothing length, sampling distance and dt must be positive");
+    if (p->iterations < 0) return fail(c, PK_ERR_ARG, "iterations must be >= 0");
+    if (p->smoothing_length / p->sampling_distance > 64.0f)
+        return fail(c, PK_ERR_ARG, "smoothing length / sampling distance too large");
+    return PK_OK;
+}
+
+int check_list(pk_ctx* c, int n, const int* index, const int* elements, int cap, long long total)
+{
+    if (n > 0 && (!index || !elements)) return fail(c, PK_ERR_ARG, "null neighbour list");
+    if (cap < 0) return fail(c, PK_ERR_ARG, "negative cap");
+    if (cap == 0 && total < 0) return fail(c, PK_ERR_ARG, "negative list total");
+    return PK_OK;
+}
+
+}  // namespace
+
+namespace pk {
+
+void prof_begin(pk_ctx* c, int kind, cudaStream_t st)
+{
+    if (!c->prof) return;
+    auto& ev = c->prof_ev[kind];
+    int u = c->prof_used[kind];
+    while ((int)ev.size() < u + 2) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        ev.push_back(e);
+    }
+    cudaEventRecord(ev[u], st);
+}
+
+void prof_end(pk_ctx* c, int kind, cudaStream_t st)
+{
+    if (!c->prof) return;
+    auto& ev = c->prof_ev[kind];
+    int u = c->prof_used[kind];
+    if ((int)ev.size() < u + 2) return;
+    cudaEventRecord(ev[u + 1], st);
+    c->prof_used[kind] = u + 2;
+}
+
+}  // namespace pk
+
+// ======================================================================
+// context
+
+PK_API int pk_ctx_create(pk_ctx** out, int device)
+{
+    if (!out) return PK_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return PK_ERR_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return PK_ERR_CUDA;
+    pk_ctx* c = new pk_ctx();
+    c->device = device;
+    if (cudaMalloc((void**)&c->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
+        delete c;
+        return PK_ERR_NOMEM;
+    }
+    *out = c;
+    return PK_OK;
+}
+
+PK_API int pk_ctx_destroy(pk_ctx* c)
+{
+    if (!c) return PK_ERR_ARG;
+    cudaSetDevice(c->device);
+    void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
+                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->lam, c->rho, c->rcnt, c->tau,
+                    c->rows, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
+                    c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
+                    c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& ev : c->prof_ev)
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    delete c;
+    return PK_OK;
+}
+
+PK_API const char* pk_last_error(const pk_ctx* c)
+{
+    return c ? c->err.c_str() : "null context";
+}
+
+PK_API int pk_ctx_status(pk_ctx* c, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_ctx_status");
+    int bits = 0;
+    e = cudaMemcpy(&bits, c->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_ctx_status");
+    if (bits) {
+        cudaMemset(c->d_err, 0, sizeof(int));
+        char msg[160];
+        snprintf(msg, sizeof msg, "capacity exceeded on the device (flags 0x%x: 1=row, 2=hits>512, 4=list)", bits);
+        return fail(c, PK_ERR_CAPACITY, msg);
+    }
+    return PK_OK;
+}
+
+PK_API int pk_last_launch_count(const pk_ctx* c) { return c ? c->launches : -1; }
+
+PK_API int pk_ctx_profile(pk_ctx* c, int enable)
+{
+    if (!c) return PK_ERR_ARG;
+    c->prof = enable != 0;
+    for (int k = 0; k < PK_PROF_KINDS; ++k) c->prof_used[k] = 0;
+    return PK_OK;
+}
+
+PK_API int pk_ctx_profile_read(pk_ctx* c, int kind, double* total_ms, int* launches)
+{
+    if (!c) return PK_ERR_ARG;
+    if (kind < 0 || kind >= PK_PROF_KINDS || !total_ms || !launches)
+        return fail(c, PK_ERR_ARG, "bad profile kind or output");
+    cudaSetDevice(c->device);
+    double sum = 0.0;
+    auto& ev = c->prof_ev[kind];
+    for (int u = 0; u + 1 < c->prof_used[kind]; u += 2) {
+        cudaError_t e = cudaEventSynchronize(ev[u + 1]);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[u], ev[u + 1]);
+        if (e != cudaSuccess) return cuda_fail(c, e, "pk_ctx_profile_read");
+        sum += ms;
+    }
+    *total_ms = sum;
+    *launches = c->prof_used[kind] / 2;
+    return PK_OK;
+}
+
+// ======================================================================
+// NeighborQuery
+
+PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, int* index,
+                       int* elements, long long elements_capacity, long long* total,
+                       pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    if (n > (1 << 29)) return fail(c, PK_ERR_ARG, "more than 2^29 particles");
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    int rc = check_nq(c, p);
+    if (rc) return rc;
+    if (p->cap > 0 && elements && elements_capacity < (long long)n * p->cap)
+        return fail(c, PK_ERR_ARG, "elements capacity below n*cap");
+    if (elements && !index) return fail(c, PK_ERR_ARG, "elements given without index");
+    cudaSetDevice(c->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    pk::Grid g = pk::make_grid(p->radius, p->lo, p->hi);
+    const int row_cap = row_capacity(p);
+    if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
+        (rc = ensure_rows(c, (long long)n * row_cap)))
+        return rc;
+    c->nq_valid = false;
+    int launches = pk::sort_particles(c, const_cast<float*>(x), nullptr, nullptr, n, g, false, nullptr,
+                                      0.f, 0.f, 0.f, false, nullptr, st);
+    launches += pk::build_rows(c, n, g, p->radius, p->cap, row_cap, index, elements,
+                               elements ? elements_capacity : 0, st);
+    c->launches = launches;
+    if ((rc = check_launch(c, "pk_nq_build"))) return rc;
+    c->grid = g;
+    c->nq_n = n;
+    c->nq_cap = p->cap;
+    c->row_cap = row_cap;
+    c->nq_h = p->radius;
+    c->exported_index = index;
+    c->exported_elements = elements;
+    c->nq_valid = true;
+    if (total) {
+        if (p->cap > 0) {
+            *total = (long long)n * p->cap;
+        } else if (index) {
+            int t = 0;
+            cudaError_t e = cudaMemcpyAsync(&t, c->offs + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(c, e, "pk_nq_build");
+            *total = n > 0 ? t : 0;
+            if (elements && *total > elements_capacity) {
+                cudaMemset(c->d_err, 0, sizeof(int));
+                return fail(c, PK_ERR_CAPACITY, "dynamic neighbour list exceeds elements_capacity");
+            }
+        } else {
+            *total = 0;
+        }
+    }
+    return PK_OK;
+}
+
+PK_API int pk_nq_row_stats(pk_ctx* c, double* mean_list, double* mean_row, int* max_row,
+                           pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!c->nq_valid) return fail(c, PK_ERR_STATE, "no neighbour build on this context");
+    cudaSetDevice(c->device);
+    std::vector<int2> h((size_t)std::max(c->nq_n, 1));
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (c->nq_n > 0)
+        e = cudaMemcpyAsync(h.data(), c->rcnt, sizeof(int2) * (size_t)c->nq_n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_nq_row_stats");
+    double sa = 0, su = 0;
+    int mx = 0;
+    for (int i = 0; i < c->nq_n; ++i) {
+        sa += h[i].x;
+        su += h[i].y;
+        mx = std::max(mx, h[i].y);
+    }
+    const double n = std::max(c->nq_n, 1);
+    if (mean_list) *mean_list = sa / n;
+    if (mean_row) *mean_row = su / n;
+    if (max_row) *max_row = mx;
+    return PK_OK;
+}
+
+// ======================================================================
+// DensityPBD / SummationDensity / integrator
+
+PK_API int pk_summation_density(pk_ctx* c, const float* x, int n, const int* index,
+                                const int* elements, int cap, long long total,
+                                const pk_pbd_params* p, float* rho, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    int rc = check_pbd(c, p);
+    if (rc) return rc;
+    if ((rc = check_list(c, n, index, elements, cap, total))) return rc;
+    if (n > 0 && (!x || !rho)) return fail(c, PK_ERR_ARG, "null positions or density");
+    cudaSetDevice(c->device);
+    pk::density_generic(x, n, index, elements, cap, total, pk::make_spiky(p->smoothing_length),
+                        effective_mass(p), rho, (cudaStream_t)stream);
+    return check_launch(c, "pk_summation_density");
+}
+
+PK_API int pk_pbd_solve(pk_ctx* c, float* x, float* v, int n, const int* index, const int* elements,
+                        int cap, long long total, const pk_pbd_params* p, float* rho_out,
+                        pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    int rc = check_pbd(c, p);
+    if (rc) return rc;
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    cudaSetDevice(c->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const pk::Spiky k = pk::make_spiky(p->smoothing_length);
+    const float mass = effective_mass(p);
+    const bool own_list = c->nq_valid && n == c->nq_n &&
+                          ((index == nullptr && elements == nullptr) ||
+                           (index == c->exported_index && elements == c->exported_elements &&
+                            cap == c->nq_cap));
+    if (own_list) {
+        int l = pk::gather_state(c, x, v, n, st);
+        l += pk::pbd_fast_solve(c, n, k, mass, p->iterations, p->dt, x, v, rho_out, st);
+        c->launches = l;
+    } else {
+        if ((rc = check_list(c, n, index, elements, cap, total))) return rc;
+        if ((rc = ensure_generic(c, n))) return rc;
+        c->launches = pk::pbd_generic_solve(c, x, v, n, index, elements, cap, total, k, mass,
+                                            p->iterations, p->dt, rho_out, st);
+    }
+    return check_launch(c, "pk_pbd_solve");
+}
+
+PK_API int pk_integrate(pk_ctx* c, float* x, float* v, const float* f, int n, const float gravity[3],
+                        float dt, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    if (!gravity) return fail(c, PK_ERR_ARG, "null gravity");
+    cudaSetDevice(c->device);
+    c->launches = pk::integrate_aos(x, v, f, n, gravity, dt, (cudaStream_t)stream);
+    return check_launch(c, "pk_integrate");
+}
+
+// ======================================================================
+// BoundaryConstraint: the box SDF is evaluated on the host once per box with
+// the float expressions of DistanceToBox / DistanceToSqure / DistanceToSegment
+// (DistanceField3D.cu:14-123, K_DistanceFieldToBox :266-280), uploaded, and
+// sampled by the kernels.  Host code is built without FMA contraction.
+
+namespace {
+
+float dot3(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+float segment_distance(const float* pos, const float* lo, const float* hi)
+{
+    float seg[3], e1[3], e2[3], nseg[3];
+    for (int a = 0; a < 3; ++a) {
+        seg[a] = hi[a] - lo[a];
+        e1[a] = pos[a] - lo[a];
+        e2[a] = pos[a] - hi[a];
+        nseg[a] = -seg[a];
+    }
+    if (dot3(e1, seg) < 0.0f) return std::sqrt(dot3(e1, e1));
+    if (dot3(e2, nseg) < 0.0f) return std::sqrt(dot3(e2, e2));
+    float l1 = dot3(e1, e1);
+    float len = std::sqrt(dot3(seg, seg));
+    if (len > 1.1920929e-7f) {
+        float is = 1.0f / std::sqrt(dot3(seg, seg));
+        for (int a = 0; a < 3; ++a) seg[a] = seg[a] * is;
+    } else {
+        seg[0] = seg[1] = seg[2] = 0.0f;
+    }
+    float l2 = dot3(e1, seg);
+    return std::sqrt(l1 - l2 * l2);
+}
+
+float square_distance(const float* pos, const float* lo, const float* hi, int axis)
+{
+    float c1[3], c2[3], c3[3], c4[3], nrm[3] = {0.f, 0.f, 0.f}, lc[2], hc[2], p[2];
+    int u = axis == 0 ? 1 : 0, w = axis == 2 ? 1 : 2;  // the two in-plane axes
+    for (int a = 0; a < 3; ++a) c1[a] = c2[a] = c3[a] = c4[a] = lo[a];
+    // corners in the order of DistanceToSqure's switch
+    if (axis == 0) {
+        c2[1] = hi[1]; c3[1] = hi[1]; c3[2] = hi[2]; c4[2] = hi[2];
+    } else if (axis == 1) {
+        c2[2] = hi[2]; c3[0] = hi[0]; c3[2] = hi[2]; c4[0] = hi[0];
+    } else {
+        c2[0] = hi[0]; c3[0] = hi[0]; c3[1] = hi[1]; c4[1] = hi[1];
+    }
+    nrm[axis] = 1.0f;
+    lc[0] = lo[u]; lc[1] = lo[w]; hc[0] = hi[u]; hc[1] = hi[w]; p[0] = pos[u]; p[1] = pos[w];
+    float d1 = segment_distance(pos, c1, c2), d2 = segment_distance(pos, c2, c3);
+    float d3 = segment_distance(pos, c3, c4), d4 = segment_distance(pos, c4, c1);
+    float rel[3] = {pos[0] - c1[0], pos[1] - c1[1], pos[2] - c1[2]};
+    float d5 = std::fabs(dot3(nrm, rel));
+    if (p[0] < hc[0] && p[0] > lc[0] && p[1] < hc[1] && p[1] > lc[1]) return d5;
+    return std::fmin(std::fmin(d1, d2), std::fmin(d3, d4));
+}
+
+float box_distance(const float* pos, const float* lo, const float* hi)
+{
+    if (pos[0] < hi[0] && pos[0] > lo[0] && pos[1] < hi[1] && pos[1] > lo[1] && pos[2] < hi[2] &&
+        pos[2] > lo[2]) {
+        float dx = std::fmin(std::fabs(pos[0] - hi[0]), std::fabs(pos[0] - lo[0]));
+        float dy = std::fmin(std::fabs(pos[1] - hi[1]), std::fabs(pos[1] - lo[1]));
+        float dz = std::fmin(std::fabs(pos[2] - hi[2]), std::fabs(pos[2] - lo[2]));
+        return std::fmin(std::fmin(dx, dy), dz);
+    }
+    const float k0[3] = {lo[0], lo[1], lo[2]}, k1[3] = {hi[0], lo[1], lo[2]};
+    const float k2[3] = {hi[0], hi[1], lo[2]}, k3[3] = {lo[0], hi[1], lo[2]};
+    const float k4[3] = {lo[0], lo[1], hi[2]}, k5[3] = {hi[0], lo[1], hi[2]};
+    const float k6[3] = {hi[0], hi[1], hi[2]}, k7[3] = {lo[0], hi[1], hi[2]};
+    float x1 = square_distance(pos, k0, k7, 0), x2 = square_distance(pos, k1, k6, 0);
+    float y1 = square_distance(pos, k0, k5, 1), y2 = square_distance(pos, k3, k6, 1);
+    float z1 = square_distance(pos, k0, k2, 2), z2 = square_distance(pos, k4, k6, 2);
+    return -std::fmin(std::fmin(std::fmin(x1, x2), std::fmin(y1, y2)), std::fmin(z1, z2));
+}
+
+}  // namespace
+
+PK_API int pk_boundary_set_box(pk_ctx* c, const float lo[3], const float hi[3], float spacing,
+                               int inverted, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!lo || !hi || !(spacing > 0.0f)) return fail(c, PK_ERR_ARG, "bad box or spacing");
+    int dims[3];
+    float left[3], h[3];
+    for (int a = 0; a < 3; ++a) {
+        if (!(hi[a] > lo[a])) return fail(c, PK_ERR_ARG, "box must have hi > lo");
+        int nb = (int)std::floor((hi[a] - lo[a]) / spacing) + 10;  // setCube (:111-115)
+        float p0 = lo[a] - 5.0f * spacing, p1 = hi[a] + 5.0f * spacing;
+        left[a] = p0;
+        h[a] = (p1 - p0) * (float)(1.0 / (double)(float)(nb + 1));  // setSpace (:198)
+        dims[a] = nb + 1;
+    }
+    long long nodes = (long long)dims[0] * dims[1] * dims[2];
+    if (nodes > (1LL << 31)) return fail(c, PK_ERR_ARG, "SDF grid too large");
+    std::vector<float> data((size_t)nodes);
+    const float sign = inverted ? 1.0f : -1.0f;
+    for (int k = 0; k < dims[2]; ++k)
+        for (int j = 0; j < dims[1]; ++j)
+            for (int i = 0; i < dims[0]; ++i) {
+                float p[3] = {left[0] + (float)i * h[0], left[1] + (float)j * h[1], left[2] + (float)k * h[2]};
+                data[((size_t)k * dims[1] + j) * dims[0] + i] = sign * box_distance(p, lo, hi);
+            }
+    cudaSetDevice(c->device);
+    size_t bytes = sizeof(float) * (size_t)nodes;
+    if (bytes > c->sdf_bytes) {
+        if (c->sdf) cudaFree(c->sdf);
+        c->sdf = nullptr;
+        c->sdf_bytes = 0;
+        if (cudaMalloc((void**)&c->sdf, bytes) != cudaSuccess)
+            return fail(c, PK_ERR_NOMEM, "device allocation of the SDF failed");
+        c->sdf_bytes = bytes;
+    }
+    cudaError_t e = cudaMemcpyAsync(c->sdf, data.data(), bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_boundary_set_box");
+    for (int a = 0; a < 3; ++a) {
+        c->sdf_left[a] = left[a];
+        c->sdf_h[a] = h[a];
+        c->sdf_dims[a] = dims[a];
+        c->sdf_box_lo[a] = lo[a];
+        c->sdf_box_hi[a] = hi[a];
+    }
+    c->sdf_inverted = inverted ? 1 : 0;
+    c->has_sdf = true;
+    return PK_OK;
+}
+
+PK_API int pk_boundary_constrain(pk_ctx* c, float* x, float* v, int n, float normal_friction,
+                                 float tangential_friction, float dt, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!c->has_sdf) return fail(c, PK_ERR_STATE, "no boundary box set");
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    cudaSetDevice(c->device);
+    c->launches = pk::boundary_aos(x, v, n, pk::sdf_view(c), normal_friction, tangential_friction, dt,
+                                   (cudaStream_t)stream);
+    return check_launch(c, "pk_boundary_constrain");
+}
+
+PK_API int pk_boundary_jitter(pk_ctx* c, int n, float* out, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || (n > 0 && !out)) return fail(c, PK_ERR_ARG, "bad jitter output");
+    cudaSetDevice(c->device);
+    c->launches = pk::boundary_jitter(out, n, (cudaStream_t)stream);
+    return check_launch(c, "pk_boundary_jitter");
+}
+
+// ======================================================================
+// fused fluid step
+
+PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, float* rho_out,
+                       pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!p) return fail(c, PK_ERR_ARG, "null step parameters");
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    if (n > (1 << 29)) return fail(c, PK_ERR_ARG, "more than 2^29 particles");
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    int rc = check_nq(c, &p->nq);
+    if (rc || (rc = check_pbd(c, &p->pbd))) return rc;
+    if (p->boundary && !c->has_sdf) return fail(c, PK_ERR_STATE, "boundary requested but no box set");
+    cudaSetDevice(c->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    pk::Grid g = pk::make_grid(p->nq.radius, p->nq.lo, p->nq.hi);
+    const int row_cap = row_capacity(&p->nq);
+    if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
+        (rc = ensure_rows(c, (long long)n * row_cap)))
+        return rc;
+    pk::SdfView sv{};
+    if (p->boundary) sv = pk::sdf_view(c);
+    c->nq_valid = false;
+    // StaticBoundary::advance, then ParticleIntegrator::begin (force zeroed),
+    // NeighborQuery::compute on the current positions, integrate, DensityPBD.
+    int l = pk::sort_particles(c, x, v, nullptr, n, g, p->boundary != 0, p->boundary ? &sv : nullptr,
+                               p->normal_friction, p->tangential_friction, p->pbd.dt, true,
+                               p->gravity, st);
+    l += pk::build_rows(c, n, g, p->nq.radius, p->nq.cap, row_cap, nullptr, nullptr, 0, st);
+    l += pk::pbd_fast_solve(c, n, pk::make_spiky(p->pbd.smoothing_length), effective_mass(&p->pbd),
+                            p->pbd.iterations, p->pbd.dt, x, v, rho_out, st);
+    c->launches = l;
+    if ((rc = check_launch(c, "pk_pbf_step"))) return rc;
+    c->grid = g;
+    c->nq_n = n;
+    c->nq_cap = p->nq.cap;
+    c->row_cap = row_cap;
+    c->nq_h = p->nq.radius;
+    c->exported_index = nullptr;
+    c->exported_elements = nullptr;
+    c->nq_valid = true;
+    return PK_OK;
+}
+
+// ======================================================================
+// ElasticityModule
+
+PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const int* elements, int cap,
+                      long long total, float horizon, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    int rc = check_list(c, n, index, elements, cap, total);
+    if (rc) return rc;
+    if (!(horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
+    cudaSetDevice(c->device);
+    long long bonds = cap > 0 ? (long long)n * cap : total;
+    if (n > c->pd_cap_n) {
+        size_t m = (size_t)n;
+        if (!(regrow(c->pd_index, m) && regrow(c->pd_invK, 9 * m) && regrow(c->pd_bulk, m) &&
+              regrow(c->pd_xold, 3 * m) && regrow(c->pd_delta, 3 * m) && regrow(c->pd_w, m))) {
+            c->pd_cap_n = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of elasticity state failed");
+        }
+        c->pd_cap_n = n;
+    }
+    if (bonds > c->pd_cap_bonds) {
+        if (!(regrow(c->pd_rest_idx, (size_t)bonds) && regrow(c->pd_rest_pos, 3 * (size_t)bonds) &&
+              regrow(c->pd_alive, (size_t)bonds))) {
+            c->pd_cap_bonds = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of the rest shape failed");
+        }
+        c->pd_cap_bonds = bonds;
+    }
+    c->pd_n = n;
+    c->pd_cap = cap;
+    c->pd_total = bonds;
+    c->pd_horizon = horizon;
+    pk::pd_rest_shape(c, x, n, index, elements, cap, bonds, horizon, (cudaStream_t)stream);
+    return check_launch(c, "pk_pd_init");
+}
+
+PK_API int pk_pd_set_bulk(pk_ctx* c, const float* bulk, int n, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    if (n != c->pd_n || (n > 0 && !bulk)) return fail(c, PK_ERR_ARG, "bulk size does not match");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMemcpyAsync(c->pd_bulk, bulk, sizeof(float) * (size_t)n,
+                                    cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_pd_set_bulk");
+    return PK_OK;
+}
+
+PK_API int pk_pd_solve(pk_ctx* c, float* x, float* v, int n, const pk_pd_params* p, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!p) return fail(c, PK_ERR_ARG, "null elasticity parameters");
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    if (n != c->pd_n) return fail(c, PK_ERR_ARG, "particle count differs from pk_pd_init");
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    if (!(p->horizon > 0.0f) || !(p->dt > 0.0f) || p->iterations < 0)
+        return fail(c, PK_ERR_ARG, "bad horizon, dt or iterations");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_solve(c, x, v, n, p->horizon, p->mu, p->lambda, p->iterations, p->dt,
+                               p->break_stretch, (cudaStream_t)stream);
+    return check_launch(c, "pk_pd_solve");
+}
+
+PK_API int pk_pd_get_rest_shape(pk_ctx* c, int* rest_idx, float* rest_pos, float* inv_k, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    cudaSetDevice(c->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (rest_idx && c->pd_total > 0)
+        e = cudaMemcpyAsync(rest_idx, c->pd_rest_idx, sizeof(int) * (size_t)c->pd_total,
+                            cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && rest_pos && c->pd_total > 0)
+        e = cudaMemcpyAsync(rest_pos, c->pd_rest_pos, 3 * sizeof(float) * (size_t)c->pd_total,
+                            cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && inv_k && c->pd_n > 0)
+        e = cudaMemcpyAsync(inv_k, c->pd_invK, 9 * sizeof(float) * (size_t)c->pd_n,
+                            cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_pd_get_rest_shape");
+    return PK_OK;
+}

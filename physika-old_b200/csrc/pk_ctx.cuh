@@ -1,0 +1,93 @@
+// pk_ctx.cuh -- the context object behind the opaque pk_ctx handle.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "pk_internal.cuh"
+
+struct pk_ctx {
+    int device = 0;
+    std::string err;
+    int* d_err = nullptr;  // latched device-side conditions (kErr* bits)
+    int launches = 0;      // kernels enqueued by the last fused step
+
+    // ---- optional per-kernel-class event timing (pk_ctx_profile)
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev[PK_PROF_KINDS];  // start/stop pairs
+    int prof_used[PK_PROF_KINDS] = {0, 0, 0, 0, 0, 0};
+
+    // ---- particle-sized scratch (capacity cap_n)
+    int cap_n = 0;
+    int* perm = nullptr;
+    int* inv = nullptr;
+    int* key = nullptr;
+    int* rank = nullptr;
+    int* count = nullptr;     // hits per particle (sorted order)
+    int* count_c = nullptr;   // hits per particle (caller order, dynamic lists)
+    int* offs = nullptr;      // exclusive scan of count_c (n + 1)
+    float4* xs_pre = nullptr;
+    float4* xs0 = nullptr;
+    float4* xa = nullptr;
+    float4* xb = nullptr;
+    float4* vs = nullptr;
+    float* lam = nullptr;
+    float* rho = nullptr;
+    int2* rcnt = nullptr;
+    uint2* tau = nullptr;
+
+    // ---- rows (capacity cap_rows entries)
+    long long cap_rows = 0;
+    int* rows = nullptr;
+
+    // ---- dense cell table (capacity cap_keys entries + 2)
+    long long cap_keys = 0;
+    int* cell_cnt = nullptr;
+    int* cell_start = nullptr;
+    int* scan_part = nullptr;  // block partials of the scan
+    long long cap_part = 0;
+
+    // ---- generic-list solver scratch (caller order)
+    int cap_g = 0;
+    float* g_rho = nullptr;
+    float* g_lam = nullptr;
+    float* g_dpos = nullptr;  // 3 per particle
+    float* g_xold = nullptr;  // 3 per particle
+
+    // ---- state of the last neighbour build
+    pk::Grid grid{};
+    int nq_n = -1;
+    int nq_cap = 0;
+    int row_cap = 0;
+    float nq_h = 0.0f;
+    const int* exported_index = nullptr;
+    const int* exported_elements = nullptr;
+    bool nq_valid = false;
+
+    // ---- box boundary (BoundaryConstraint)
+    float* sdf = nullptr;
+    size_t sdf_bytes = 0;
+    float sdf_left[3] = {0, 0, 0};
+    float sdf_h[3] = {0, 0, 0};
+    float sdf_box_lo[3] = {0, 0, 0};
+    float sdf_box_hi[3] = {0, 0, 0};
+    int sdf_dims[3] = {0, 0, 0};
+    int sdf_inverted = 1;
+    bool has_sdf = false;
+
+    // ---- peridynamics (ElasticityModule) frozen state
+    int pd_n = -1;
+    int pd_cap = 0;            // layout of the rest shape (0 = CSR)
+    long long pd_total = 0;
+    int* pd_index = nullptr;   // copy of the list index (counts or offsets)
+    int* pd_rest_idx = nullptr;
+    float* pd_rest_pos = nullptr;  // 3 per bond
+    unsigned char* pd_alive = nullptr;
+    float* pd_invK = nullptr;      // 9 per particle, row-major
+    float* pd_bulk = nullptr;
+    float* pd_xold = nullptr;
+    float* pd_delta = nullptr;
+    float* pd_w = nullptr;
+    float pd_horizon = 0.0f;
+    long long pd_cap_bonds = 0;
+    int pd_cap_n = 0;
+};

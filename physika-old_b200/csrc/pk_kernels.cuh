@@ -1,0 +1,47 @@
+// pk_kernels.cuh -- host-side launchers shared between the kernel files.
+#pragma once
+#include "pk_boundary.cuh"
+#include "pk_ctx.cuh"
+
+namespace pk {
+
+// pk_api.cu: event pairs around a kernel class when profiling is on.
+void prof_begin(pk_ctx* c, int kind, cudaStream_t st);
+void prof_end(pk_ctx* c, int kind, cudaStream_t st);
+
+// pk_sort.cu
+void exclusive_scan(const int* in, long long m, int* out, int* part, cudaStream_t st);
+long long scan_parts_needed(long long m);
+int scan_launches();
+int sort_particles(pk_ctx* c, float* x, float* v, const float* f, int n, const Grid& g,
+                   bool boundary, const SdfView* sdf, float nfric, float tfric, float dt,
+                   bool integrate, const float grav[3], cudaStream_t st);
+
+// pk_nbr.cu: the cap-nearest selection and the row emission over the sorted
+// particles.  pub_index/pub_elements may be null.  Returns kernels launched.
+int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap,
+               int* pub_index, int* pub_elements, long long pub_capacity, cudaStream_t st);
+
+// pk_pbd.cu
+int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
+                   float* x, float* v, float* rho_out, cudaStream_t st);
+int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, const int* elements,
+                      int cap, long long total, const Spiky& k, float mass, int iterations,
+                      float dt, float* rho_out, cudaStream_t st);
+int density_generic(const float* x, int n, const int* index, const int* elements, int cap,
+                    long long total, const Spiky& k, float mass, float* rho, cudaStream_t st);
+int gather_state(pk_ctx* c, const float* x, const float* v, int n, cudaStream_t st);
+int integrate_aos(float* x, float* v, const float* f, int n, const float g[3], float dt,
+                  cudaStream_t st);
+int boundary_aos(float* x, float* v, int n, const SdfView& s, float nfric, float tfric, float dt,
+                 cudaStream_t st);
+SdfView sdf_view(const pk_ctx* c);
+int boundary_jitter(float* out, int n, cudaStream_t st);
+
+// pk_pd.cu
+int pd_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int* elements,
+                  int cap, long long total, float horizon, cudaStream_t st);
+int pd_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, float lambda,
+             int iterations, float dt, float break_stretch, cudaStream_t st);
+
+}  // namespace pk

@@ -1,0 +1,407 @@
+// pk_pbd.cu -- DensityPBD (with SummationDensity) and ParticleIntegrator.
+//
+// Fast path: the rows built by pk_nbr.cu in sorted space.  One Jacobi
+// iteration of the reference (DensityPBD::takeOneIteration,
+// DensityPBD.cu:305-365: density, lambdas, displacement with atomics,
+// position update) is two gather passes here:
+//   pass A: rho_i and lambda_i over N(i) (K_ComputeDensity
+//           SummationDensity.cu:13-36 + K_ComputeLambdas DensityPBD.cu:46-90),
+//   pass B: x_i' = x_i + sum over the row of m_ij * dp_ij, m_ij = [j in N(i)]
+//           + [i in N(j)] -- the same sum the reference's scatter
+//           (+dp_ij to i, -dp_ij to j, DensityPBD.cu:134-179) accumulates,
+//           since dp_ji = -dp_ij bit for bit.
+// G lanes share one particle: each takes every G-th row entry, partial sums
+// are combined with xor shuffles.  x is ping-ponged (Jacobi).
+#include "pk_kernels.cuh"
+
+namespace pk {
+
+constexpr unsigned kAll = 0xffffffffu;
+
+template <int G>
+__device__ __forceinline__ float group_sum(float v)
+{
+#pragma unroll
+    for (int off = G / 2; off >= 1; off >>= 1) v += __shfl_xor_sync(kAll, v, off);
+    return v;
+}
+
+template <int G>
+__global__ void __launch_bounds__(256)
+    k_pass_density(const float4* __restrict__ xs, const int* __restrict__ rows,
+                   const int2* __restrict__ rcnt, int row_cap, int n, Spiky k, float mass,
+                   float* __restrict__ lam, float* __restrict__ rho_out)
+{
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = gid / G, sub = gid % G;
+    const bool valid = s < n;
+    float rho = 0.f, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    if (valid) {
+        const float4 xi = xs[s];
+        const int na = rcnt[s].x;
+        const int* row = rows + (long long)s * row_cap;
+        for (int e = sub; e < na; e += G) {
+            const int j = __ldg(row + e) & kRowIndexMask;
+            const float4 xj = __ldg(xs + j);
+            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+            float w, g;
+            spiky_wg(k, r, w, g);
+            rho += mass * w;
+            if (r > kEpsilon) {
+                const float ir = 1.0f / r;
+                const float g0 = g * dx * ir, g1 = g * dy * ir, g2 = g * dz * ir;
+                gx += g0;
+                gy += g1;
+                gz += g2;
+                sg += g0 * g0 + g1 * g1 + g2 * g2;
+            }
+        }
+    }
+    rho = group_sum<G>(rho);
+    sg = group_sum<G>(sg);
+    gx = group_sum<G>(gx);
+    gy = group_sum<G>(gy);
+    gz = group_sum<G>(gz);
+    if (valid && sub == 0) {
+        float l = sg + (gx * gx + gy * gy + gz * gz);
+        l = -(rho - 1000.0f) / (l + 0.1f);  // rest density hard-coded (DensityPBD.cu:87)
+        lam[s] = l > 0.0f ? 0.0f : l;
+        if (rho_out != nullptr) rho_out[s] = rho;
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256)
+    k_pass_disp(const float4* __restrict__ xs, const float* __restrict__ lam,
+                const int* __restrict__ rows, const int2* __restrict__ rcnt, int row_cap, int n,
+                Spiky k, float4* __restrict__ xs_out)
+{
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = gid / G, sub = gid % G;
+    const bool valid = s < n;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+        xi = xs[s];
+        const float li = lam[s];
+        const int nu = rcnt[s].y;
+        const int* row = rows + (long long)s * row_cap;
+        for (int e = sub; e < nu; e += G) {
+            const int v = __ldg(row + e);
+            const int j = v & kRowIndexMask;
+            const float mult = (float)(((unsigned)v >> 31) + (((unsigned)v >> 30) & 1u));
+            const float4 xj = __ldg(xs + j);
+            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+            if (r > kEpsilon) {
+                float w, g;
+                spiky_wg(k, r, w, g);
+                const float sl = li + __ldg(lam + j);
+                const float ir = 1.0f / r;
+                // 10*(x_i - x_j)*(lambda_i + lambda_j)*grad*(1/r) (DensityPBD.cu:158)
+                ax += mult * (10.0f * dx * sl * g * ir);
+                ay += mult * (10.0f * dy * sl * g * ir);
+                az += mult * (10.0f * dz * sl * g * ir);
+            }
+        }
+    }
+    ax = group_sum<G>(ax);
+    ay = group_sum<G>(ay);
+    az = group_sum<G>(az);
+    if (valid && sub == 0) xs_out[s] = make_float4(xi.x + ax, xi.y + ay, xi.z + az, 0.f);
+}
+
+// Sorted -> caller order: x, v += (x - x_old)/dt (DP_UpdateVelocity,
+// DensityPBD.cu:367-378), outDensity.
+__global__ void __launch_bounds__(256)
+    k_finish(const float4* __restrict__ xf, const float4* __restrict__ x0, const float4* __restrict__ vs,
+             const float* __restrict__ rho_s, const int* __restrict__ perm, int n, float dt,
+             float* __restrict__ x, float* __restrict__ v, float* __restrict__ rho_out)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int i = perm[s];
+    float4 p = xf[s], q = x0[s], u = vs[s];
+    x[3 * i] = p.x;
+    x[3 * i + 1] = p.y;
+    x[3 * i + 2] = p.z;
+    v[3 * i] = u.x + (p.x - q.x) / dt;
+    v[3 * i + 1] = u.y + (p.y - q.y) / dt;
+    v[3 * i + 2] = u.z + (p.z - q.z) / dt;
+    if (rho_out != nullptr) rho_out[i] = rho_s[s];
+}
+
+// Caller order -> sorted: the solver's starting state.
+__global__ void __launch_bounds__(256)
+    k_gather_state(const float* __restrict__ x, const float* __restrict__ v, const int* __restrict__ perm,
+                   int n, float4* __restrict__ xs0, float4* __restrict__ vs)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int i = perm[s];
+    xs0[s] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.f);
+    vs[s] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f);
+}
+
+constexpr int kGroup = 8;
+
+int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
+                   float* x, float* v, float* rho_out, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const unsigned nb1 = (unsigned)((n + 255) / 256);
+    const unsigned nbg = (unsigned)(((long long)n * kGroup + 255) / 256);
+    int launches = 0;
+    const float4* cur = c->xs0;
+    for (int it = 0; it < iterations; ++it) {
+        float4* nxt = (it & 1) ? c->xb : c->xa;
+        const bool last = it == iterations - 1;
+        prof_begin(c, PK_PROF_DENSITY, st);
+        k_pass_density<kGroup><<<nbg, 256, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, k, mass,
+                                                    c->lam, last ? c->rho : nullptr);
+        prof_end(c, PK_PROF_DENSITY, st);
+        prof_begin(c, PK_PROF_DISP, st);
+        k_pass_disp<kGroup><<<nbg, 256, 0, st>>>(cur, c->lam, c->rows, c->rcnt, c->row_cap, n, k, nxt);
+        prof_end(c, PK_PROF_DISP, st);
+        cur = nxt;
+        launches += 2;
+    }
+    prof_begin(c, PK_PROF_FINISH, st);
+    k_finish<<<nb1, 256, 0, st>>>(cur, c->xs0, c->vs, c->rho, c->perm, n, dt, x, v,
+                                  (rho_out != nullptr && iterations > 0) ? rho_out : nullptr);
+    prof_end(c, PK_PROF_FINISH, st);
+    return launches + 1;
+}
+
+int gather_state(pk_ctx* c, const float* x, const float* v, int n, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_gather_state<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, v, c->perm, n, c->xs0, c->vs);
+    return 1;
+}
+
+// ------------------------------------------------------------------------
+// Generic path: any NeighborList<int> in caller order (a list that did not
+// come from this context's pk_nq_build).  One thread per particle, the
+// displacement scattered with atomics as in the reference.
+
+__device__ __forceinline__ int nb_size(const int* index, int cap, long long total, int n, int i)
+{
+    // NeighborList::getNeighborSize (NeighborList.h:27-41)
+    if (cap > 0) return index[i];
+    if (i >= n - 1) return (int)(total - index[i]);
+    return index[i + 1] - index[i];
+}
+__device__ __forceinline__ long long nb_at(const int* index, int cap, int i, int k)
+{
+    return cap > 0 ? (long long)cap * i + k : (long long)index[i] + k;
+}
+
+__global__ void __launch_bounds__(256)
+    k_g_density(const float* __restrict__ x, int n, const int* __restrict__ index,
+                const int* __restrict__ elements, int cap, long long total, Spiky k, float mass,
+                float* __restrict__ rho)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2], acc = 0.f;
+    int m = nb_size(index, cap, total, n, i);
+    for (int e = 0; e < m; ++e) {
+        int j = elements[nb_at(index, cap, i, e)];
+        float dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz), w, g;
+        spiky_wg(k, r, w, g);
+        acc += mass * w;
+    }
+    rho[i] = acc;
+}
+
+__global__ void __launch_bounds__(256)
+    k_g_lambda(const float* __restrict__ x, const float* __restrict__ rho, int n,
+               const int* __restrict__ index, const int* __restrict__ elements, int cap,
+               long long total, Spiky k, float* __restrict__ lam, float* __restrict__ dpos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+    float sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    int m = nb_size(index, cap, total, n, i);
+    for (int e = 0; e < m; ++e) {
+        int j = elements[nb_at(index, cap, i, e)];
+        float dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (r > kEpsilon) {
+            float w, g;
+            spiky_wg(k, r, w, g);
+            float ir = 1.0f / r;
+            float g0 = g * dx * ir, g1 = g * dy * ir, g2 = g * dz * ir;
+            gx += g0; gy += g1; gz += g2;
+            sg += g0 * g0 + g1 * g1 + g2 * g2;
+        }
+    }
+    float l = sg + (gx * gx + gy * gy + gz * gz);
+    l = -(rho[i] - 1000.0f) / (l + 0.1f);
+    lam[i] = l > 0.0f ? 0.0f : l;
+    dpos[3 * i] = 0.f;  // m_deltaPos.reset() (DensityPBD.cu:315)
+    dpos[3 * i + 1] = 0.f;
+    dpos[3 * i + 2] = 0.f;
+}
+
+__global__ void __launch_bounds__(256)
+    k_g_disp(const float* __restrict__ x, const float* __restrict__ lam, int n,
+             const int* __restrict__ index, const int* __restrict__ elements, int cap,
+             long long total, Spiky k, float* __restrict__ dpos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2], li = lam[i];
+    int m = nb_size(index, cap, total, n, i);
+    for (int e = 0; e < m; ++e) {
+        int j = elements[nb_at(index, cap, i, e)];
+        float dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (r > kEpsilon) {
+            float w, g;
+            spiky_wg(k, r, w, g);
+            float sl = li + lam[j], ir = 1.0f / r;
+            float p0 = 10.0f * dx * sl * g * ir, p1 = 10.0f * dy * sl * g * ir,
+                  p2 = 10.0f * dz * sl * g * ir;
+            atomicAdd(dpos + 3 * i, p0);
+            atomicAdd(dpos + 3 * j, -p0);
+            atomicAdd(dpos + 3 * i + 1, p1);
+            atomicAdd(dpos + 3 * j + 1, -p1);
+            atomicAdd(dpos + 3 * i + 2, p2);
+            atomicAdd(dpos + 3 * j + 2, -p2);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_g_add(float* __restrict__ x, const float* __restrict__ d, long long m)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) x[t] += d[t];
+}
+
+__global__ void __launch_bounds__(256)
+    k_g_velocity(float* __restrict__ v, const float* __restrict__ x, const float* __restrict__ xold,
+                 long long m, float dt)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) v[t] += (x[t] - xold[t]) / dt;
+}
+
+int density_generic(const float* x, int n, const int* index, const int* elements, int cap,
+                    long long total, const Spiky& k, float mass, float* rho, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_g_density<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho);
+    return 1;
+}
+
+int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, const int* elements,
+                      int cap, long long total, const Spiky& k, float mass, int iterations,
+                      float dt, float* rho_out, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const long long m3 = 3LL * n;
+    const unsigned nb3 = (unsigned)((m3 + 255) / 256);
+    int launches = 0;
+    cudaMemcpyAsync(c->g_xold, x, sizeof(float) * (size_t)m3, cudaMemcpyDeviceToDevice, st);
+    float* rho = rho_out != nullptr ? rho_out : c->g_rho;
+    for (int it = 0; it < iterations; ++it) {
+        k_g_density<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho);
+        k_g_lambda<<<nb, 256, 0, st>>>(x, rho, n, index, elements, cap, total, k, c->g_lam, c->g_dpos);
+        k_g_disp<<<nb, 256, 0, st>>>(x, c->g_lam, n, index, elements, cap, total, k, c->g_dpos);
+        k_g_add<<<nb3, 256, 0, st>>>(x, c->g_dpos, m3);
+        launches += 4;
+    }
+    k_g_velocity<<<nb3, 256, 0, st>>>(v, x, c->g_xold, m3, dt);
+    return launches + 1;
+}
+
+// ------------------------------------------------ integrator and boundary
+
+__global__ void __launch_bounds__(256)
+    k_integrate(float* __restrict__ x, float* __restrict__ v, const float* __restrict__ f, int n,
+                float gx, float gy, float gz, float dt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float g[3] = {gx, gy, gz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float fa = f != nullptr ? f[3 * i + a] : 0.f;
+        float va = v[3 * i + a] + dt * (fa + g[a]);  // K_UpdateVelocity (ParticleIntegrator.cu:69)
+        v[3 * i + a] = va;
+        x[3 * i + a] += dt * va;                     // K_UpdatePosition (ParticleIntegrator.cu:111)
+    }
+}
+
+int integrate_aos(float* x, float* v, const float* f, int n, const float g[3], float dt, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_integrate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, v, f, n, g[0], g[1], g[2], dt);
+    return 1;
+}
+
+__global__ void __launch_bounds__(256)
+    k_boundary(float* __restrict__ x, float* __restrict__ v, int n, SdfView s, float nfric,
+               float tfric, float dt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 p = make_float3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+    float3 u = make_float3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    if (sdf_constrain(s, i, p, u, nfric, tfric, dt)) {
+        x[3 * i] = p.x; x[3 * i + 1] = p.y; x[3 * i + 2] = p.z;
+        v[3 * i] = u.x; v[3 * i + 1] = u.y; v[3 * i + 2] = u.z;
+    }
+}
+
+int boundary_aos(float* x, float* v, int n, const SdfView& s, float nfric, float tfric, float dt,
+                 cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_boundary<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, v, n, s, nfric, tfric, dt);
+    return 1;
+}
+
+__global__ void __launch_bounds__(256) k_jitter(float* __restrict__ out, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    curandState st;
+    curand_init((unsigned long long)i, 0ull, 0ull, &st);
+    out[i] = curand_uniform(&st);
+}
+
+int boundary_jitter(float* out, int n, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_jitter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, n);
+    return 1;
+}
+
+SdfView sdf_view(const pk_ctx* c)
+{
+    SdfView s{};
+    s.data = c->sdf;
+    float mh = 0.f;
+    for (int a = 0; a < 3; ++a) {
+        s.left[a] = c->sdf_left[a];
+        s.inv_h[a] = (float)(1.0 / (double)c->sdf_h[a]);
+        s.box_lo[a] = c->sdf_box_lo[a];
+        s.box_hi[a] = c->sdf_box_hi[a];
+        mh = fmaxf(mh, c->sdf_h[a]);
+    }
+    s.margin = 2.0f * mh + 1e-6f;
+    s.nx = c->sdf_dims[0];
+    s.ny = c->sdf_dims[1];
+    s.nz = c->sdf_dims[2];
+    s.inverted = c->sdf_inverted;
+    return s;
+}
+
+}  // namespace pk

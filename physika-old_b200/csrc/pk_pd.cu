@@ -1,0 +1,348 @@
+// pk_pd.cu -- ElasticityModule (projective peridynamics).
+//
+// The rest shape (bond list + rest positions) is frozen at initialisation
+// (ElasticityModule::resetRestShape, ElasticityModule.cu:496-517), so K^-1 is
+// computed once here; the reference recomputes the same matrix every step
+// (solveElasticity -> computeInverseK, :404-411).  Each projection iteration
+// is EM_EnforceElasticity (:123-242) + K_UpdatePosition (:281-292).
+#include "pk_kernels.cuh"
+
+namespace pk {
+
+__device__ __forceinline__ int pd_size(const int* index, int cap, long long total, int n, int i)
+{
+    if (cap > 0) return index[i];
+    if (i >= n - 1) return (int)(total - index[i]);
+    return index[i + 1] - index[i];
+}
+__device__ __forceinline__ long long pd_at(const int* index, int cap, int i, int k)
+{
+    return cap > 0 ? (long long)cap * i + k : (long long)index[i] + k;
+}
+
+// K_UpdateRestShape (ElasticityModule.cu:449-494): copy the list, self to slot 0.
+__global__ void __launch_bounds__(256)
+    k_pd_rest(const float* __restrict__ x, int n, const int* __restrict__ index,
+              const int* __restrict__ elements, int cap, long long total,
+              int* __restrict__ ridx, float* __restrict__ rpos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int m = pd_size(index, cap, total, n, i);
+    for (int e = 0; e < m; ++e) {
+        long long at = pd_at(index, cap, i, e);
+        int j = elements[at];
+        if (i != j || e == 0) {
+            ridx[at] = j;
+            rpos[3 * at] = x[3 * j];
+            rpos[3 * at + 1] = x[3 * j + 1];
+            rpos[3 * at + 2] = x[3 * j + 2];
+        } else {
+            long long a0 = pd_at(index, cap, i, 0);
+            ridx[at] = ridx[a0];
+            rpos[3 * at] = rpos[3 * a0];
+            rpos[3 * at + 1] = rpos[3 * a0 + 1];
+            rpos[3 * at + 2] = rpos[3 * a0 + 2];
+            ridx[a0] = j;
+            rpos[3 * a0] = x[3 * j];
+            rpos[3 * a0 + 1] = x[3 * j + 1];
+            rpos[3 * a0 + 2] = x[3 * j + 2];
+        }
+    }
+}
+
+// CorrectedKernel / SmoothKernel (Kernel.h:68-75,99-142).
+__device__ __forceinline__ float smooth_w(float r, float h)
+{
+    float q = r / h;
+    return q > 1.0f ? 0.0f : (1.0f - q * q);
+}
+__device__ __forceinline__ float corr_w(float r, float h)
+{
+    float q = r / h;
+    return q * q * q * smooth_w(r, h);
+}
+__device__ __forceinline__ float corr_wrr(float r, float h)
+{
+    float q = r / h;
+    return q * smooth_w(r, h) / (h * h);
+}
+
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations in double.
+__device__ void jacobi3(double A[3][3], double Q[3][3], double w[3])
+{
+    for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) Q[p][q] = (p == q) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
+        if (off < 1e-300) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                double apq = A[p][q];
+                if (fabs(apq) < 1e-300) continue;
+                double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int r = 0; r < 3; ++r) {
+                    double arp = A[r][p], arq = A[r][q];
+                    A[r][p] = c * arp - s * arq;
+                    A[r][q] = s * arp + c * arq;
+                }
+                for (int r = 0; r < 3; ++r) {
+                    double apr = A[p][r], aqr = A[q][r];
+                    A[p][r] = c * apr - s * aqr;
+                    A[q][r] = s * apr + c * aqr;
+                }
+                for (int r = 0; r < 3; ++r) {
+                    double qrp = Q[r][p], qrq = Q[r][q];
+                    Q[r][p] = c * qrp - s * qrq;
+                    Q[r][q] = s * qrp + c * qrq;
+                }
+            }
+    }
+    for (int p = 0; p < 3; ++p) w[p] = A[p][p];
+}
+
+// EM_PrecomputeShape (ElasticityModule.cu:21-116): weighted second moment of
+// the rest bonds, then the pseudo-inverse with singular values <= 1e-4*h
+// replaced by 1 (polarDecomposition's SVD of a symmetric PSD matrix is its
+// eigen-decomposition).  invK row-major.
+__global__ void __launch_bounds__(128)
+    k_pd_invk(int n, const int* __restrict__ index, int cap, long long total,
+              const float* __restrict__ rpos, float h, float* __restrict__ invK)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long a0 = pd_at(index, cap, i, 0);
+    float ri0 = rpos[3 * a0], ri1 = rpos[3 * a0 + 1], ri2 = rpos[3 * a0 + 2];
+    int m = pd_size(index, cap, total, n, i);
+    float M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, tw = 0.f;
+    for (int e = 0; e < m; ++e) {
+        long long at = pd_at(index, cap, i, e);
+        float q0 = rpos[3 * at] - ri0, q1 = rpos[3 * at + 1] - ri1, q2 = rpos[3 * at + 2] - ri2;
+        float r = sqrtf(q0 * q0 + q1 * q1 + q2 * q2);
+        if (r > kEpsilon) {
+            float wt = corr_w(r, h), sw = sqrtf(wt);
+            float q[3] = {q0 / h * sw, q1 / h * sw, q2 / h * sw};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) M[a][b] += q[a] * q[b];
+            tw += wt;
+        }
+    }
+    if (tw > kEpsilon) {
+        float s = 1.0f / tw;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) M[a][b] *= s;
+    }
+    double A[3][3], Q[3][3], w[3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) A[a][b] = (double)M[a][b];
+    jacobi3(A, Q, w);
+    double thr = (double)(0.0001f * h);
+    for (int a = 0; a < 3; ++a) {
+        double sv = fabs(w[a]);
+        w[a] = sv > thr ? 1.0 / sv : 1.0;
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            invK[9LL * i + 3 * a + b] =
+                (float)(Q[a][0] * w[0] * Q[b][0] + Q[a][1] * w[1] * Q[b][1] + Q[a][2] * w[2] * Q[b][2]);
+}
+
+__global__ void __launch_bounds__(256) k_fill_f(float* __restrict__ p, long long m, float v)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) p[t] = v;
+}
+__global__ void __launch_bounds__(256) k_fill_u8(unsigned char* __restrict__ p, long long m, unsigned char v)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) p[t] = v;
+}
+
+__device__ __forceinline__ void normalize_or_zero(float& a, float& b, float& c)
+{
+    // v.norm() > EPSILON ? v.normalize() : 0 (ElasticityModule.cu:211-212);
+    // normalize() is 0 below FLT_EPSILON (vector_3d.inl:220-224).
+    float l = sqrtf(a * a + b * b + c * c);
+    if (l > kEpsilon && l > 1.1920928955078125e-7f) {
+        float is = 1.0f / l;
+        a *= is; b *= is; c *= is;
+    } else {
+        a = b = c = 0.f;
+    }
+}
+
+// EM_EnforceElasticity (ElasticityModule.cu:123-242); `alive` masks broken bonds.
+__global__ void __launch_bounds__(128)
+    k_pd_enforce(const float* __restrict__ x, int n, const int* __restrict__ index, int cap,
+                 long long total, const int* __restrict__ ridx, const float* __restrict__ rpos,
+                 const unsigned char* __restrict__ alive, const float* __restrict__ invK,
+                 const float* __restrict__ bulk, float horizon, float mu, float lambda,
+                 float* __restrict__ delta, float* __restrict__ wts)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long a0 = pd_at(index, cap, i, 0);
+    const float ri0 = rpos[3 * a0], ri1 = rpos[3 * a0 + 1], ri2 = rpos[3 * a0 + 2];
+    const float ci0 = x[3 * i], ci1 = x[3 * i + 1], ci2 = x[3 * i + 2];
+    const int m = pd_size(index, cap, total, n, i);
+    const float bulk_i = bulk[i];
+    float F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, tw = 0.f;
+    for (int e = 0; e < m; ++e) {
+        long long at = pd_at(index, cap, i, e);
+        if (!alive[at]) continue;
+        int j = ridx[at];
+        float e0 = rpos[3 * at] - ri0, e1 = rpos[3 * at + 1] - ri1, e2 = rpos[3 * at + 2] - ri2;
+        float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        if (r > kEpsilon) {
+            float wt = corr_w(r, horizon);
+            float p[3] = {(x[3 * j] - ci0) / horizon, (x[3 * j + 1] - ci1) / horizon,
+                          (x[3 * j + 2] - ci2) / horizon};
+            float q[3] = {e0 / horizon * wt, e1 / horizon * wt, e2 / horizon * wt};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) F[a][b] += p[a] * q[b];
+            tw += wt;
+        }
+    }
+    if (tw > kEpsilon) {
+        float s = 1.0f / tw, G[3][3];
+        const float* K = invK + 9LL * i;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) F[a][b] *= s;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) G[a][b] = F[a][0] * K[b] + F[a][1] * K[3 + b] + F[a][2] * K[6 + b];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) F[a][b] = G[a][b];
+    }
+    float det = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    if (det < -0.001f) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) F[a][b] = (a == b) ? 1.f : 0.f;
+    }
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, accA = 0.f;
+    for (int e = 0; e < m; ++e) {
+        long long at = pd_at(index, cap, i, e);
+        if (!alive[at]) continue;
+        int j = ridx[at];
+        float e0 = ri0 - rpos[3 * at], e1 = ri1 - rpos[3 * at + 1], e2 = ri2 - rpos[3 * at + 2];
+        float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        if (!(r > 0.01f * horizon)) continue;
+        float xj0 = x[3 * j], xj1 = x[3 * j + 1], xj2 = x[3 * j + 2];
+        float rd0 = F[0][0] * e0 + F[0][1] * e1 + F[0][2] * e2;
+        float rd1 = F[1][0] * e0 + F[1][1] * e1 + F[1][2] * e2;
+        float rd2 = F[2][0] * e0 + F[2][1] * e1 + F[2][2] * e2;
+        float cd0 = ci0 - xj0, cd1 = ci1 - xj1, cd2 = ci2 - xj2;
+        normalize_or_zero(cd0, cd1, cd2);
+        normalize_or_zero(rd0, rd1, rd2);
+        float wrr = corr_wrr(r, horizon);
+        float mu_ij = mu * bulk_i * wrr, la_ij = lambda * bulk_i * wrr, dw = mu_ij + la_ij;
+        // mu/lambda targets for i (x_j + r*dir) and for j (x_i - r*dir)
+        float d0 = mu_ij * (xj0 + r * rd0) + la_ij * (xj0 + r * cd0);
+        float d1 = mu_ij * (xj1 + r * rd1) + la_ij * (xj1 + r * cd1);
+        float d2 = mu_ij * (xj2 + r * rd2) + la_ij * (xj2 + r * cd2);
+        float b0 = mu_ij * (ci0 - r * rd0) + la_ij * (ci0 - r * cd0);
+        float b1 = mu_ij * (ci1 - r * rd1) + la_ij * (ci1 - r * cd1);
+        float b2 = mu_ij * (ci2 - r * rd2) + la_ij * (ci2 - r * cd2);
+        accA += dw;
+        acc0 += d0; acc1 += d1; acc2 += d2;
+        atomicAdd(wts + j, dw);
+        atomicAdd(delta + 3 * j, b0);
+        atomicAdd(delta + 3 * j + 1, b1);
+        atomicAdd(delta + 3 * j + 2, b2);
+    }
+    atomicAdd(wts + i, accA);
+    atomicAdd(delta + 3 * i, acc0);
+    atomicAdd(delta + 3 * i + 1, acc1);
+    atomicAdd(delta + 3 * i + 2, acc2);
+}
+
+// K_UpdatePosition (ElasticityModule.cu:281-292): x = (x_old + delta)/(1 + w).
+__global__ void __launch_bounds__(256)
+    k_pd_update(float* __restrict__ x, const float* __restrict__ xold, const float* __restrict__ delta,
+                const float* __restrict__ wts, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float den = 1.0f + wts[i];
+    x[3 * i] = (xold[3 * i] + delta[3 * i]) / den;
+    x[3 * i + 1] = (xold[3 * i + 1] + delta[3 * i + 1]) / den;
+    x[3 * i + 2] = (xold[3 * i + 2] + delta[3 * i + 2]) / den;
+}
+
+__global__ void __launch_bounds__(256)
+    k_pd_velocity(float* __restrict__ v, const float* __restrict__ x, const float* __restrict__ xold,
+                  long long m, float dt)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) v[t] += (x[t] - xold[t]) / dt;
+}
+
+// Stretch break (no reference counterpart): a bond dies for good once
+// |x_i - x_j| > (1 + s) * |rest_i - rest_j|.
+__global__ void __launch_bounds__(256)
+    k_pd_break(const float* __restrict__ x, int n, const int* __restrict__ index, int cap,
+               long long total, const int* __restrict__ ridx, const float* __restrict__ rpos,
+               unsigned char* __restrict__ alive, float s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long a0 = pd_at(index, cap, i, 0);
+    int m = pd_size(index, cap, total, n, i);
+    for (int e = 0; e < m; ++e) {
+        long long at = pd_at(index, cap, i, e);
+        if (!alive[at]) continue;
+        int j = ridx[at];
+        float r0 = rpos[3 * at] - rpos[3 * a0], r1 = rpos[3 * at + 1] - rpos[3 * a0 + 1],
+              r2 = rpos[3 * at + 2] - rpos[3 * a0 + 2];
+        float c0 = x[3 * j] - x[3 * i], c1 = x[3 * j + 1] - x[3 * i + 1], c2 = x[3 * j + 2] - x[3 * i + 2];
+        float lr = sqrtf(r0 * r0 + r1 * r1 + r2 * r2), lc = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+        if (lc > (1.0f + s) * lr) alive[at] = 0;
+    }
+}
+
+int pd_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int* elements, int cap,
+                  long long total, float horizon, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    long long bonds = cap > 0 ? (long long)n * cap : total;
+    cudaMemcpyAsync(c->pd_index, index, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    k_pd_rest<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, c->pd_rest_idx, c->pd_rest_pos);
+    k_pd_invk<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, c->pd_index, cap, total, c->pd_rest_pos,
+                                                          horizon, c->pd_invK);
+    k_fill_f<<<nb, 256, 0, st>>>(c->pd_bulk, n, 1.0f);  // computeMaterialStiffness (:371-387)
+    if (bonds > 0)
+        k_fill_u8<<<(unsigned)((bonds + 255) / 256), 256, 0, st>>>(c->pd_alive, bonds, 1);
+    return 5;
+}
+
+int pd_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, float lambda,
+             int iterations, float dt, float break_stretch, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const unsigned nb = (unsigned)((n + 255) / 256), nb128 = (unsigned)((n + 127) / 128);
+    const long long m3 = 3LL * n;
+    int launches = 0;
+    cudaMemcpyAsync(c->pd_xold, x, sizeof(float) * (size_t)m3, cudaMemcpyDeviceToDevice, st);
+    if (break_stretch > 0.f) {
+        k_pd_break<<<nb, 256, 0, st>>>(x, n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_idx,
+                                       c->pd_rest_pos, c->pd_alive, break_stretch);
+        ++launches;
+    }
+    for (int it = 0; it < iterations; ++it) {
+        cudaMemsetAsync(c->pd_delta, 0, sizeof(float) * (size_t)m3, st);
+        cudaMemsetAsync(c->pd_w, 0, sizeof(float) * (size_t)n, st);
+        k_pd_enforce<<<nb128, 128, 0, st>>>(x, n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_idx,
+                                            c->pd_rest_pos, c->pd_alive, c->pd_invK, c->pd_bulk,
+                                            horizon, mu, lambda, c->pd_delta, c->pd_w);
+        k_pd_update<<<nb, 256, 0, st>>>(x, c->pd_xold, c->pd_delta, c->pd_w, n);
+        launches += 2;
+    }
+    k_pd_velocity<<<(unsigned)((m3 + 255) / 256), 256, 0, st>>>(v, x, c->pd_xold, m3, dt);
+    return launches + 1;
+}
+
+}  // namespace pk

@@ -1,0 +1,277 @@
+// pk_sort.cu -- counting sort of particles into blocked-Morton cells.
+//
+// Replaces GridHash::construct (GridHash.cu:297-323): the reference counts
+// with atomics, reduces on the host, scans and scatters ids with atomics (the
+// order inside a cell is whatever the atomics produce), and re-mallocs `ids`
+// every build.  Here: one pass computes key + in-cell rank (optionally after
+// the boundary projection), a device-wide scan gives cell starts (no host
+// round trip), a scatter places ids, and a per-cell fix-up sorts each cell's
+// ids ascending so the order is deterministic.  A final gather builds the
+// sorted float4 arrays the list build and the solver read.
+#include "pk_boundary.cuh"
+#include "pk_kernels.cuh"
+
+namespace pk {
+
+Grid make_grid(float h, const float lo[3], const float hi[3])
+{
+    // GridHash::setSpace (GridHash.cu:46-75), float arithmetic as on the host.
+    Grid g;
+    const int padding = 2;
+    g.ds = h;
+    int n[3];
+    for (int a = 0; a < 3; ++a) {
+        float pad = (float)padding * h;
+        float nseg = (hi[a] - lo[a]) / h;
+        g.lo[a] = lo[a] - pad;
+        n[a] = (int)(ceilf(nseg) + 1.0f + (float)(2 * padding));
+    }
+    g.nx = n[0];
+    g.ny = n[1];
+    g.nz = n[2];
+    g.bx = (g.nx + 3) / 4;
+    g.by = (g.ny + 3) / 4;
+    g.bz = (g.nz + 3) / 4;
+    g.nkeys = (long long)g.bx * g.by * g.bz * 64;
+    return g;
+}
+
+Spiky make_spiky(float h)
+{
+    Spiky k;
+    k.h = h;
+    k.inv_h = 1.0f / h;
+    float hh = h * h;
+    k.cw = 15.0f / ((float)M_PI * hh * h);
+    k.cg = -45.0f / ((float)M_PI * hh * h);
+    return k;
+}
+
+// key = blocked-Morton cell key, or nkeys for particles outside the grid
+// (the reference leaves those out of the hash, GridHash.cu:85,194; they still
+// query).  rank = arrival order inside the cell.
+template <bool kBoundary>
+__global__ void __launch_bounds__(256) k_keys(float* __restrict__ x, float* __restrict__ v, int n,
+                                              Grid g, int* __restrict__ key,
+                                              int* __restrict__ rank, int* __restrict__ cell_cnt,
+                                              SdfView sdf, float nfric, float tfric, float dt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 p = make_float3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+    if (kBoundary) {
+        float3 u = make_float3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        if (sdf_constrain(sdf, i, p, u, nfric, tfric, dt)) {
+            x[3 * i] = p.x; x[3 * i + 1] = p.y; x[3 * i + 2] = p.z;
+            v[3 * i] = u.x; v[3 * i + 1] = u.y; v[3 * i + 2] = u.z;
+        }
+    }
+    int3 c = cell3(g, p.x, p.y, p.z);
+    int k = cell_key(g, c.x, c.y, c.z);
+    if (k < 0) k = (int)g.nkeys;
+    key[i] = k;
+    rank[i] = atomicAdd(&cell_cnt[k], 1);
+}
+
+// ---------------------------------------------------------------- scan
+// Exclusive scan of in[0..m) into out[0..m], out[m] = total.  Three passes:
+// tile sums, a one-block scan of the sums, tile scans with the carried offset.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* smem_warp, int& total)
+{
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) smem_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        int w = lane < nw ? smem_warp[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, wi, off);
+            if (lane >= off) wi += y;
+        }
+        if (lane < nw) smem_warp[lane] = wi - w;
+        if (lane == nw - 1) smem_warp[32] = wi;
+    }
+    __syncthreads();
+    int res = smem_warp[warp] + incl - v;
+    total = smem_warp[32];
+    __syncthreads();
+    return res;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restrict__ in, long long m,
+                                                              int* __restrict__ part)
+{
+    __shared__ int sw[33];
+    long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < m) s += in[base + k];
+    int tot;
+    block_exclusive_scan(s, sw, tot);
+    if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_parts(int* __restrict__ part, int nparts)
+{
+    __shared__ int sw[33];
+    int carry = 0;
+    for (int base = 0; base < nparts; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < nparts ? part[i] : 0;
+        int tot;
+        int ex = block_exclusive_scan(v, sw, tot);
+        if (i < nparts) part[i] = ex + carry;
+        carry += tot;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_down(const int* __restrict__ in, long long m,
+                                                            const int* __restrict__ part,
+                                                            int* __restrict__ out)
+{
+    __shared__ int sw[33];
+    long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int vals[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        vals[k] = base + k < m ? in[base + k] : 0;
+        s += vals[k];
+    }
+    int tot;
+    int ex = block_exclusive_scan(s, sw, tot) + part[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < m) out[base + k] = ex;
+        ex += vals[k];
+    }
+    if (base < m && base + kScanItems >= m) out[m] = ex;  // the thread holding the last item
+}
+
+int scan_launches() { return 3; }
+
+void exclusive_scan(const int* in, long long m, int* out, int* part, cudaStream_t st)
+{
+    long long nparts = (m + kScanTile - 1) / kScanTile;
+    if (nparts < 1) nparts = 1;
+    k_scan_reduce<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part);
+    k_scan_parts<<<1, 1024, 0, st>>>(part, (int)nparts);
+    k_scan_down<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, out);
+}
+
+long long scan_parts_needed(long long m) { return (m + kScanTile - 1) / kScanTile + 1; }
+
+// ------------------------------------------------------- scatter + fix-up
+
+__global__ void __launch_bounds__(256) k_scatter(const int* __restrict__ key, const int* __restrict__ rank,
+                                                 const int* __restrict__ start, int n,
+                                                 int* __restrict__ perm)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    perm[start[key[i]] + rank[i]] = i;
+}
+
+// Sorts the ids of each cell ascending (insertion sort; cells hold ~10-30).
+// Buckets above 2048 entries (only the "outside the grid" bucket can be that
+// large) keep their atomic order.
+__global__ void __launch_bounds__(256) k_fix_cells(const int* __restrict__ start, long long ncells,
+                                                   int* __restrict__ perm)
+{
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int a = start[c], b = start[c + 1];
+    int m = b - a;
+    if (m < 2 || m > 2048) return;
+    int* p = perm + a;
+    for (int u = 1; u < m; ++u) {
+        int t = p[u];
+        int w = u - 1;
+        while (w >= 0 && p[w] > t) {
+            p[w + 1] = p[w];
+            --w;
+        }
+        p[w + 1] = t;
+    }
+}
+
+// Sorted-order gather: xs_pre = positions the list is built on; when
+// kIntegrate, also ParticleIntegrator::integrate (ParticleIntegrator.cu:59-70,
+// 102-112) into xs0/vs: v += dt*(f + g), x += dt*v.
+template <bool kIntegrate>
+__global__ void __launch_bounds__(256) k_gather(const float* __restrict__ x, const float* __restrict__ v,
+                                                const float* __restrict__ f,
+                                                const int* __restrict__ perm, int n,
+                                                float4* __restrict__ xs_pre, float4* __restrict__ xs0,
+                                                float4* __restrict__ vs, int* __restrict__ inv,
+                                                float gx, float gy, float gz, float dt)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int i = perm[s];
+    float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+    xs_pre[s] = make_float4(px, py, pz, 0.0f);
+    inv[i] = s;
+    if (kIntegrate) {
+        float vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        if (f) { fx = f[3 * i]; fy = f[3 * i + 1]; fz = f[3 * i + 2]; }
+        vx += dt * (fx + gx);
+        vy += dt * (fy + gy);
+        vz += dt * (fz + gz);
+        xs0[s] = make_float4(px + dt * vx, py + dt * vy, pz + dt * vz, 0.0f);
+        vs[s] = make_float4(vx, vy, vz, 0.0f);
+    }
+}
+
+// ------------------------------------------------------------------ host
+
+int sort_particles(pk_ctx* c, float* x, float* v, const float* f, int n, const Grid& g,
+                   bool boundary, const SdfView* sdf, float nfric, float tfric, float dt,
+                   bool integrate, const float grav[3], cudaStream_t st)
+{
+    int launches = 0;
+    long long nk = g.nkeys + 1;  // + the "outside" bucket
+    prof_begin(c, PK_PROF_SORT, st);
+    cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (size_t)nk, st);
+    unsigned nb = (unsigned)((n + 255) / 256);
+    SdfView sv{};
+    if (sdf) sv = *sdf;
+    if (n > 0) {
+        if (boundary)
+            k_keys<true><<<nb, 256, 0, st>>>(x, v, n, g, c->key, c->rank, c->cell_cnt, sv, nfric, tfric, dt);
+        else
+            k_keys<false><<<nb, 256, 0, st>>>(x, v, n, g, c->key, c->rank, c->cell_cnt, sv, nfric, tfric, dt);
+        ++launches;
+    }
+    exclusive_scan(c->cell_cnt, nk, c->cell_start, c->scan_part, st);
+    launches += scan_launches();
+    if (n > 0) {
+        k_scatter<<<nb, 256, 0, st>>>(c->key, c->rank, c->cell_start, n, c->perm);
+        k_fix_cells<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(c->cell_start, nk, c->perm);
+        if (integrate)
+            k_gather<true><<<nb, 256, 0, st>>>(x, v, f, c->perm, n, c->xs_pre, c->xs0, c->vs, c->inv,
+                                               grav[0], grav[1], grav[2], dt);
+        else
+            k_gather<false><<<nb, 256, 0, st>>>(x, v, f, c->perm, n, c->xs_pre, nullptr, nullptr,
+                                                c->inv, 0.f, 0.f, 0.f, 0.f);
+        launches += 3;
+    }
+    prof_end(c, PK_PROF_SORT, st);
+    return launches;
+}
+
+}  // namespace pk

@@ -1,0 +1,266 @@
+"""Python binding of libpkhot.so (include/pk_hot.h) through ctypes.
+
+Torch is used only for device memory and streams: every call passes raw
+device pointers of contiguous float32/int32 CUDA tensors plus the current
+CUDA stream to the C ABI.  There is no CPU fallback: if the library is not
+built, or no GPU is present, the calls raise.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpkhot.so")
+
+PK_OK, PK_ERR_ARG, PK_ERR_CUDA, PK_ERR_CAPACITY, PK_ERR_STATE, PK_ERR_NOMEM = range(6)
+
+EXPORTED = [
+    "pk_ctx_create", "pk_ctx_destroy", "pk_last_error", "pk_ctx_status", "pk_last_launch_count",
+    "pk_ctx_profile", "pk_ctx_profile_read",
+    "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
+    "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
+    "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
+]
+
+
+class PkError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pk error {code}: {msg}")
+        self.code = code
+
+
+class NqParams(ctypes.Structure):
+    _fields_ = [("radius", ctypes.c_float), ("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3),
+                ("cap", ctypes.c_int), ("max_neighbors", ctypes.c_int)]
+
+
+class PbdParams(ctypes.Structure):
+    _fields_ = [("smoothing_length", ctypes.c_float), ("sampling_distance", ctypes.c_float),
+                ("rest_density", ctypes.c_float), ("iterations", ctypes.c_int), ("dt", ctypes.c_float)]
+
+
+class PbfParams(ctypes.Structure):
+    _fields_ = [("nq", NqParams), ("pbd", PbdParams), ("gravity", ctypes.c_float * 3),
+                ("boundary", ctypes.c_int), ("normal_friction", ctypes.c_float),
+                ("tangential_friction", ctypes.c_float)]
+
+
+class PdParams(ctypes.Structure):
+    _fields_ = [("horizon", ctypes.c_float), ("mu", ctypes.c_float), ("lambda_", ctypes.c_float),
+                ("iterations", ctypes.c_int), ("dt", ctypes.c_float), ("break_stretch", ctypes.c_float)]
+
+
+_lib = None
+
+
+def load():
+    """Loads libpkhot.so and declares the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is not built (run __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, F, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_longlong
+    sig = {
+        "pk_ctx_create": ([ctypes.POINTER(P), I], I),
+        "pk_ctx_destroy": ([P], I),
+        "pk_last_error": ([P], ctypes.c_char_p),
+        "pk_ctx_status": ([P, P], I),
+        "pk_last_launch_count": ([P], I),
+        "pk_ctx_profile": ([P, I], I),
+        "pk_ctx_profile_read": ([P, I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I)], I),
+        "pk_nq_build": ([P, P, I, ctypes.POINTER(NqParams), P, P, LL, ctypes.POINTER(LL), P], I),
+        "pk_nq_row_stats": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                             ctypes.POINTER(I), P], I),
+        "pk_summation_density": ([P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
+        "pk_pbd_solve": ([P, P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
+        "pk_integrate": ([P, P, P, P, I, ctypes.POINTER(F * 3), F, P], I),
+        "pk_boundary_set_box": ([P, ctypes.POINTER(F * 3), ctypes.POINTER(F * 3), F, I, P], I),
+        "pk_boundary_constrain": ([P, P, P, I, F, F, F, P], I),
+        "pk_boundary_jitter": ([P, I, P, P], I),
+        "pk_pbf_step": ([P, P, P, I, ctypes.POINTER(PbfParams), P, P], I),
+        "pk_pd_init": ([P, P, I, P, P, I, LL, F, P], I),
+        "pk_pd_set_bulk": ([P, P, I, P], I),
+        "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
+        "pk_pd_get_rest_shape": ([P, P, P, P, P], I),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _f3(v):
+    return (ctypes.c_float * 3)(*[float(a) for a in v])
+
+
+def nq_params(radius, lo, hi, cap, max_neighbors=0):
+    return NqParams(float(radius), _f3(lo), _f3(hi), int(cap), int(max_neighbors))
+
+
+def pbd_params(smoothing_length, sampling_distance, rest_density=1000.0, iterations=5, dt=1e-3):
+    return PbdParams(float(smoothing_length), float(sampling_distance), float(rest_density),
+                     int(iterations), float(dt))
+
+
+def pbf_params(nq, pbd, gravity=(0.0, -9.8, 0.0), boundary=True, normal_friction=0.95,
+               tangential_friction=0.0):
+    return PbfParams(nq, pbd, _f3(gravity), int(bool(boundary)), float(normal_friction),
+                     float(tangential_friction))
+
+
+class Context:
+    """One pk_ctx: the module scratch of NeighborQuery/DensityPBD/ElasticityModule."""
+
+    def __init__(self, device=0):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("pkhot needs a CUDA device; there is no CPU path")
+        self.L = load()
+        self.device = device
+        torch.cuda.set_device(device)
+        h = ctypes.c_void_p()
+        rc = self.L.pk_ctx_create(ctypes.byref(h), device)
+        if rc != PK_OK:
+            raise PkError(rc, "pk_ctx_create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pk_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != PK_OK:
+            raise PkError(rc, self.L.pk_last_error(self.h).decode())
+
+    def status(self):
+        return self.L.pk_ctx_status(self.h, _stream())
+
+    def check_status(self):
+        self._check(self.status())
+
+    def launch_count(self):
+        return self.L.pk_last_launch_count(self.h)
+
+    PROF_KINDS = ("sort", "select", "emit", "density", "disp", "finish")
+
+    def profile(self, enable=True):
+        self._check(self.L.pk_ctx_profile(self.h, int(bool(enable))))
+
+    def profile_read(self):
+        """{kind: (total_ms, launches)} of the kernel classes since profile(True)."""
+        out = {}
+        for k, name in enumerate(self.PROF_KINDS):
+            ms, nl = ctypes.c_double(), ctypes.c_int()
+            self._check(self.L.pk_ctx_profile_read(self.h, k, ctypes.byref(ms), ctypes.byref(nl)))
+            out[name] = (ms.value, nl.value)
+        return out
+
+    # ---- NeighborQuery
+    def nq_build(self, x, radius, lo, hi, cap, max_neighbors=0, want_list=True):
+        """Returns (index, elements, total) as the reference's NeighborList."""
+        import torch
+        n = x.shape[0]
+        p = nq_params(radius, lo, hi, cap, max_neighbors)
+        tot = ctypes.c_longlong(0)
+        if not want_list:
+            self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), None, None, 0,
+                                           None, _stream()))
+            return None, None, 0
+        index = torch.empty(max(n, 1), dtype=torch.int32, device=x.device)
+        if cap > 0:
+            elements = torch.full((max(n * cap, 1),), -1, dtype=torch.int32, device=x.device)
+            self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index),
+                                           _ptr(elements), n * cap, ctypes.byref(tot), _stream()))
+            return index[:n], elements, tot.value
+        # dynamic: size first, then fill (the reference also reads the total back)
+        self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index), None, 0,
+                                       ctypes.byref(tot), _stream()))
+        elements = torch.empty(max(tot.value, 1), dtype=torch.int32, device=x.device)
+        self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index),
+                                       _ptr(elements), tot.value, ctypes.byref(tot), _stream()))
+        return index[:n], elements[: tot.value], tot.value
+
+    def row_stats(self):
+        """(mean capped-list length incl. self, mean solver-row length, longest row)."""
+        a, u, m = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(self.L.pk_nq_row_stats(self.h, ctypes.byref(a), ctypes.byref(u), ctypes.byref(m),
+                                           _stream()))
+        return a.value, u.value, m.value
+
+    # ---- DensityPBD / SummationDensity
+    def summation_density(self, x, index, elements, cap, total, params):
+        import torch
+        n = x.shape[0]
+        rho = torch.empty(max(n, 1), dtype=torch.float32, device=x.device)
+        self._check(self.L.pk_summation_density(self.h, _ptr(x), n, _ptr(index), _ptr(elements), cap,
+                                                total, ctypes.byref(params), _ptr(rho), _stream()))
+        return rho[:n]
+
+    def pbd_solve(self, x, v, index, elements, cap, total, params, rho_out=None):
+        self._check(self.L.pk_pbd_solve(self.h, _ptr(x), _ptr(v), x.shape[0], _ptr(index),
+                                        _ptr(elements), cap, total, ctypes.byref(params),
+                                        _ptr(rho_out), _stream()))
+
+    def integrate(self, x, v, gravity, dt, f=None):
+        self._check(self.L.pk_integrate(self.h, _ptr(x), _ptr(v), _ptr(f), x.shape[0],
+                                        ctypes.byref(_f3(gravity)), float(dt), _stream()))
+
+    # ---- boundary
+    def boundary_set_box(self, lo, hi, spacing, inverted=True):
+        self._check(self.L.pk_boundary_set_box(self.h, ctypes.byref(_f3(lo)), ctypes.byref(_f3(hi)),
+                                               float(spacing), int(bool(inverted)), _stream()))
+
+    def boundary_constrain(self, x, v, dt, normal_friction=0.95, tangential_friction=0.0):
+        self._check(self.L.pk_boundary_constrain(self.h, _ptr(x), _ptr(v), x.shape[0],
+                                                 float(normal_friction), float(tangential_friction),
+                                                 float(dt), _stream()))
+
+    def boundary_jitter(self, n):
+        import torch
+        out = torch.empty(max(n, 1), dtype=torch.float32, device=f"cuda:{self.device}")
+        self._check(self.L.pk_boundary_jitter(self.h, n, _ptr(out), _stream()))
+        return out[:n]
+
+    # ---- fused step
+    def pbf_step(self, x, v, params, rho_out=None):
+        self._check(self.L.pk_pbf_step(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(params),
+                                       _ptr(rho_out), _stream()))
+
+    # ---- ElasticityModule
+    def pd_init(self, x, index, elements, cap, total, horizon):
+        self._check(self.L.pk_pd_init(self.h, _ptr(x), x.shape[0], _ptr(index), _ptr(elements), cap,
+                                      total, float(horizon), _stream()))
+
+    def pd_set_bulk(self, bulk):
+        self._check(self.L.pk_pd_set_bulk(self.h, _ptr(bulk), bulk.shape[0], _stream()))
+
+    def pd_solve(self, x, v, horizon, mu=0.05, lam=0.1, iterations=10, dt=1e-3, break_stretch=0.0):
+        p = PdParams(float(horizon), float(mu), float(lam), int(iterations), float(dt), float(break_stretch))
+        self._check(self.L.pk_pd_solve(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(p), _stream()))
+
+    def pd_get_rest_shape(self, rest_idx=None, rest_pos=None, inv_k=None):
+        self._check(self.L.pk_pd_get_rest_shape(self.h, _ptr(rest_idx), _ptr(rest_pos), _ptr(inv_k),
+                                                _stream()))

@@ -1,0 +1,130 @@
+"""DensityPBD / ParticleIntegrator / boundary parity against the CPU
+restatement.  Tolerance: positions within 1e-5 relative (2-norm over all
+particles) for one solve, 1e-4 after 1 and 10 full steps; the FP32 sums are
+taken in a different order than the reference's atomics, so bit equality is
+not expected.  Densities within 1e-5 relative."""
+import numpy as np
+import pytest
+import torch
+
+import pkhot
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def t(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def prepared(oracle, seed=0, n_side=16):
+    sc = scenes.dam_break_small(seed=seed, n_side=n_side)
+    v0 = np.random.default_rng(seed).normal(0, 0.05, sc.x.shape).astype(np.float32)
+    return sc, v0
+
+
+@pytest.mark.parametrize("cap", [60, 0])
+def test_pbd_solve_own_list(ctx, oracle, cap):
+    sc, v0 = prepared(oracle)
+    x, v = t(sc.x), t(v0)
+    idx, el, tot = ctx.nq_build(x, sc.radius, sc.lo, sc.hi, cap)
+    ctx.integrate(x, v, sc.gravity, sc.dt)
+    prm = pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt)
+    rho = torch.zeros(x.shape[0], device="cuda")
+    ctx.pbd_solve(x, v, idx, el, cap, tot, prm, rho)
+    ctx.check_status()
+    ri, re = oracle.neighbor_query(sc.x, sc.radius, sc.lo, sc.hi, cap)
+    xo, vo = oracle.integrate(sc.x, v0, sc.gravity, sc.dt)
+    f, m = oracle.density_scaling(sc.spacing, sc.radius, 1000.0)
+    xo, vo, ro = oracle.pbd_constrain(xo, vo, ri, re, cap, sc.radius, f * m, 5, sc.dt)
+    assert rel(x.cpu().numpy(), xo) < 1e-5
+    assert rel(v.cpu().numpy(), vo) < 1e-4
+    assert rel(rho.cpu().numpy(), ro) < 1e-5
+
+
+def test_pbd_solve_foreign_list(ctx, oracle):
+    # a list that did not come from this context: the generic path
+    sc, v0 = prepared(oracle, seed=1)
+    ri, re = oracle.neighbor_query(sc.x, sc.radius, sc.lo, sc.hi, 60)
+    x, v = t(sc.x), t(v0)
+    prm = pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt)
+    ctx.pbd_solve(x, v, t(ri).int(), t(re).int(), 60, ri.shape[0] * 60, prm)
+    ctx.check_status()
+    f, m = oracle.density_scaling(sc.spacing, sc.radius, 1000.0)
+    xo, vo, _ = oracle.pbd_constrain(sc.x, v0, ri, re, 60, sc.radius, f * m, 5, sc.dt)
+    assert rel(x.cpu().numpy(), xo) < 1e-5
+
+
+def test_summation_density(ctx, oracle):
+    sc, _ = prepared(oracle, seed=2)
+    ri, re = oracle.neighbor_query(sc.x, sc.radius, sc.lo, sc.hi, 0)
+    prm = pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt)
+    rho = ctx.summation_density(t(sc.x), t(ri).int(), t(re).int(), 0, re.shape[0], prm)
+    f, m = oracle.density_scaling(sc.spacing, sc.radius, 1000.0)
+    ro = oracle.summation_density(sc.x, ri, re, 0, sc.radius, f * m)
+    assert rel(rho.cpu().numpy(), ro) < 1e-6
+
+
+def oracle_step(oracle, sc, sdf, rnd, x, v):
+    x, v = oracle.sdf_constrain(x, v, sdf, rnd, 0.95, 0.0, sc.dt)
+    ri, re = oracle.neighbor_query(x, sc.radius, sc.lo, sc.hi, sc.cap)
+    x, v = oracle.integrate(x, v, sc.gravity, sc.dt)
+    f, m = oracle.density_scaling(sc.spacing, sc.radius, sc.rest_density)
+    return oracle.pbd_constrain(x, v, ri, re, sc.cap, sc.radius, f * m, sc.iterations, sc.dt)
+
+
+def test_fused_step_1_and_10(ctx, oracle):
+    sc = scenes.dam_break_small(seed=0)
+    # start slightly below the floor so the boundary acts from step 1
+    x0 = sc.x.copy()
+    x0[:, 1] -= 0.0052
+    v0 = np.zeros_like(x0)
+    ctx.boundary_set_box(sc.lo, sc.hi, sc.sdf_spacing, True)
+    rnd = ctx.boundary_jitter(x0.shape[0]).cpu().numpy()
+    sdf = oracle.sdf_box(sc.lo, sc.hi, sc.sdf_spacing, True)
+    x, v = t(x0), t(v0)
+    prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
+                           pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt), sc.gravity)
+    xo, vo = x0, v0
+    for step in range(10):
+        ctx.pbf_step(x, v, prm)
+        xo, vo, _ = oracle_step(oracle, sc, sdf, rnd, xo, vo)
+        if step in (0, 9):
+            ctx.check_status()
+            assert rel(x.cpu().numpy(), xo) < 1e-4, step
+            assert rel(v.cpu().numpy(), vo) < 1e-3, step
+    assert np.all(x.cpu().numpy()[:, 1] > 0.0)
+
+
+def test_fused_step_equals_module_calls(ctx, oracle):
+    sc = scenes.dam_break_small(seed=3, n_side=20)
+    ctx.boundary_set_box(sc.lo, sc.hi, sc.sdf_spacing, True)
+    x1, v1 = t(sc.x), t(sc.v)
+    x2, v2 = t(sc.x), t(sc.v)
+    prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
+                           pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt), sc.gravity)
+    for _ in range(3):
+        ctx.pbf_step(x1, v1, prm)
+        ctx.boundary_constrain(x2, v2, sc.dt)
+        idx, el, tot = ctx.nq_build(x2, sc.radius, sc.lo, sc.hi, sc.cap)
+        ctx.integrate(x2, v2, sc.gravity, sc.dt)
+        ctx.pbd_solve(x2, v2, idx, el, sc.cap, tot, prm.pbd)
+    ctx.check_status()
+    assert rel(x1.cpu().numpy(), x2.cpu().numpy().astype(np.float64)) < 1e-6
+
+
+def test_argument_errors(ctx):
+    x = t(np.zeros((4, 3), np.float32))
+    with pytest.raises(pkhot.PkError) as e:
+        ctx.nq_build(x, -1.0, (0, 0, 0), (1, 1, 1), 8)
+    assert e.value.code == pkhot.PK_ERR_ARG
+    with pytest.raises(pkhot.PkError) as e:
+        ctx.pbd_solve(x, x, None, None, 8, 0, pkhot.pbd_params(0.01, 0.005, 1000, 5, -1.0))
+    assert e.value.code == pkhot.PK_ERR_ARG
+    with pytest.raises(pkhot.PkError) as e:
+        ctx.pd_solve(x, x, 0.01)  # before pd_init on a fresh context
+    assert e.value.code in (pkhot.PK_ERR_STATE, pkhot.PK_ERR_ARG)
