@@ -121,9 +121,20 @@ int pk_pbd_solve(pk_ctx* ctx, float* x, float* v, int n, const int* index,
 
 /* ParticleIntegrator::integrate (Dynamics/ParticleSystem/ParticleIntegrator.cu:128-138):
  * v += dt*(f + g) (K_UpdateVelocity :59-70), then x += dt*v (K_UpdatePosition
- * :102-112).  f may be NULL (ParticleIntegrator::begin zeroes it, :32). */
+ * :102-112).  f may be NULL (ParticleIntegrator::begin zeroes it, :32).  x may
+ * be NULL: then only the velocity update runs (updateVelocity, :86-100). */
 int pk_integrate(pk_ctx* ctx, float* x, float* v, const float* f, int n,
                  const float gravity[3], float dt, pk_stream stream);
+
+/* ParticleIntegrator::updatePosition alone (K_UpdatePosition,
+ * ParticleIntegrator.cu:102-112): x += dt*v. */
+int pk_advect(pk_ctx* ctx, float* x, const float* v, int n, float dt, pk_stream stream);
+
+/* v += (x - x_old)/dt: DensityPBD::updateVelocity (DP_UpdateVelocity,
+ * DensityPBD.cu:367-392) and ElasticityModule::updateVelocity (K_UpdateVelocity,
+ * ElasticityModule.cu:295-306,423-437). */
+int pk_update_velocity(pk_ctx* ctx, float* v, const float* x, const float* x_old, int n,
+                       float dt, pk_stream stream);
 
 /* ------------------------------------------------- BoundaryConstraint */
 

@@ -321,12 +321,6 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
         (rc = ensure_rows(c, (long long)n * row_cap)))
         return rc;
     c->nq_valid = false;
-    int launches = pk::sort_particles(c, const_cast<float*>(x), nullptr, nullptr, n, g, false, nullptr,
-                                      0.f, 0.f, 0.f, false, nullptr, st);
-    launches += pk::build_rows(c, n, g, p->radius, p->cap, row_cap, index, elements,
-                               elements ? elements_capacity : 0, st);
-    c->launches = launches;
-    if ((rc = check_launch(c, "pk_nq_build"))) return rc;
     c->grid = g;
     c->nq_n = n;
     c->nq_cap = p->cap;
@@ -334,6 +328,12 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
     c->nq_h = p->radius;
     c->exported_index = index;
     c->exported_elements = elements;
+    int launches = pk::sort_particles(c, const_cast<float*>(x), nullptr, nullptr, n, g, false, nullptr,
+                                      0.f, 0.f, 0.f, false, nullptr, st);
+    launches += pk::build_rows(c, n, g, p->radius, p->cap, row_cap, index, elements,
+                               elements ? elements_capacity : 0, st);
+    c->launches = launches;
+    if ((rc = check_launch(c, "pk_nq_build"))) return rc;
     c->nq_valid = true;
     if (total) {
         if (p->cap > 0) {
@@ -436,11 +436,31 @@ PK_API int pk_integrate(pk_ctx* c, float* x, float* v, const float* f, int n, co
 {
     if (!c) return PK_ERR_ARG;
     if (n < 0) return fail(c, PK_ERR_ARG, "negative particle count");
-    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    if (n > 0 && !v) return fail(c, PK_ERR_ARG, "null velocities");
     if (!gravity) return fail(c, PK_ERR_ARG, "null gravity");
     cudaSetDevice(c->device);
     c->launches = pk::integrate_aos(x, v, f, n, gravity, dt, (cudaStream_t)stream);
     return check_launch(c, "pk_integrate");
+}
+
+PK_API int pk_advect(pk_ctx* c, float* x, const float* v, int n, float dt, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || (n > 0 && (!x || !v))) return fail(c, PK_ERR_ARG, "bad positions or velocities");
+    cudaSetDevice(c->device);
+    c->launches = pk::advect_aos(x, v, n, dt, (cudaStream_t)stream);
+    return check_launch(c, "pk_advect");
+}
+
+PK_API int pk_update_velocity(pk_ctx* c, float* v, const float* x, const float* x_old, int n, float dt,
+                              pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || (n > 0 && (!x || !v || !x_old))) return fail(c, PK_ERR_ARG, "bad arrays");
+    if (!(dt > 0.0f)) return fail(c, PK_ERR_ARG, "dt must be positive");
+    cudaSetDevice(c->device);
+    c->launches = pk::velocity_from_positions(v, x, x_old, n, dt, (cudaStream_t)stream);
+    return check_launch(c, "pk_update_velocity");
 }
 
 // ======================================================================
@@ -615,7 +635,16 @@ PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params
         return rc;
     pk::SdfView sv{};
     if (p->boundary) sv = pk::sdf_view(c);
+    // The build state is recorded before anything is launched: the solver
+    // passes read the row stride from the context.
     c->nq_valid = false;
+    c->grid = g;
+    c->nq_n = n;
+    c->nq_cap = p->nq.cap;
+    c->row_cap = row_cap;
+    c->nq_h = p->nq.radius;
+    c->exported_index = nullptr;
+    c->exported_elements = nullptr;
     // StaticBoundary::advance, then ParticleIntegrator::begin (force zeroed),
     // NeighborQuery::compute on the current positions, integrate, DensityPBD.
     int l = pk::sort_particles(c, x, v, nullptr, n, g, p->boundary != 0, p->boundary ? &sv : nullptr,
@@ -626,13 +655,6 @@ PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params
                             p->pbd.iterations, p->pbd.dt, x, v, rho_out, st);
     c->launches = l;
     if ((rc = check_launch(c, "pk_pbf_step"))) return rc;
-    c->grid = g;
-    c->nq_n = n;
-    c->nq_cap = p->nq.cap;
-    c->row_cap = row_cap;
-    c->nq_h = p->nq.radius;
-    c->exported_index = nullptr;
-    c->exported_elements = nullptr;
     c->nq_valid = true;
     return PK_OK;
 }

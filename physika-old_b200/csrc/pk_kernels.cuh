@@ -33,6 +33,8 @@ int density_generic(const float* x, int n, const int* index, const int* elements
 int gather_state(pk_ctx* c, const float* x, const float* v, int n, cudaStream_t st);
 int integrate_aos(float* x, float* v, const float* f, int n, const float g[3], float dt,
                   cudaStream_t st);
+int advect_aos(float* x, const float* v, int n, float dt, cudaStream_t st);
+int velocity_from_positions(float* v, const float* x, const float* xold, int n, float dt, cudaStream_t st);
 int boundary_aos(float* x, float* v, int n, const SdfView& s, float nfric, float tfric, float dt,
                  cudaStream_t st);
 SdfView sdf_view(const pk_ctx* c);

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(256)
         float fa = f != nullptr ? f[3 * i + a] : 0.f;
         float va = v[3 * i + a] + dt * (fa + g[a]);  // K_UpdateVelocity (ParticleIntegrator.cu:69)
         v[3 * i + a] = va;
-        x[3 * i + a] += dt * va;                     // K_UpdatePosition (ParticleIntegrator.cu:111)
+        if (x != nullptr) x[3 * i + a] += dt * va;  // K_UpdatePosition (ParticleIntegrator.cu:111)
     }
 }
 
@@ -343,6 +343,29 @@ int integrate_aos(float* x, float* v, const float* f, int n, const float g[3], f
 {
     if (n <= 0) return 0;
     k_integrate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, v, f, n, g[0], g[1], g[2], dt);
+    return 1;
+}
+
+__global__ void __launch_bounds__(256) k_advect(float* __restrict__ x, const float* __restrict__ v,
+                                                long long m, float dt)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) x[t] += dt * v[t];
+}
+
+int advect_aos(float* x, const float* v, int n, float dt, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    long long m = 3LL * n;
+    k_advect<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, v, m, dt);
+    return 1;
+}
+
+int velocity_from_positions(float* v, const float* x, const float* xold, int n, float dt, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    long long m = 3LL * n;
+    k_g_velocity<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(v, x, xold, m, dt);
     return 1;
 }
 

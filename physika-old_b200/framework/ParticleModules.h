@@ -1,0 +1,266 @@
+// ParticleModules.h -- the hot-path modules with the reference's class names,
+// fields and public methods, each backed by the sm_100a C ABI (pk_hot.h):
+//   NeighborQuery       Framework/Topology/NeighborQuery.h:12-95
+//   SummationDensity    Dynamics/ParticleSystem/SummationDensity.h:14-67
+//   DensityPBD          Dynamics/ParticleSystem/DensityPBD.h:17-88
+//   ParticleIntegrator  Dynamics/ParticleSystem/ParticleIntegrator.h:7-54
+//   ElasticityModule    Dynamics/ParticleSystem/ElasticityModule.h:18-107
+//   BoundaryConstraint  Dynamics/ParticleSystem/BoundaryConstraint.h (box SDF)
+// and the models/nodes that wire them (PositionBasedFluidModel.cpp:41-101,
+// Peridynamics.cpp:29-80, ParticleFluid, ParticleElasticBody.cpp:15-98,
+// StaticBoundary.cpp:45-94).
+#pragma once
+#include "Node.h"
+
+namespace PhysIKA {
+
+template <typename TDataType>
+class NeighborQuery : public ComputeModule {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+
+    NeighborQuery();
+    NeighborQuery(Real s, Coord lo, Coord hi);
+    ~NeighborQuery() override = default;
+
+    void compute() override;
+    void setBoundingBox(Coord lowerBound, Coord upperBound);
+    void queryParticleNeighbors(NeighborList<int>& nbr, DeviceArray<Coord>& pos, Real radius);
+    void setNeighborSizeLimit(int num) { m_maxNum = num; }
+
+    DEF_EMPTY_IN_VAR(Radius, Real, "Search radius");
+    DEF_EMPTY_IN_ARRAY(Position, Coord, DeviceType::GPU, "Particle position");
+    DEF_EMPTY_OUT_NEIGHBOR_LIST(Neighborhood, int, "Neighboring particles' ids");
+
+protected:
+    bool initializeImpl() override;
+
+private:
+    void query(NeighborList<int>& nbr, DeviceArray<Coord>& pos, Real h);
+    int m_maxNum = 0;
+    Coord m_lowBound, m_highBound;
+};
+
+template <typename TDataType>
+class SummationDensity : public ComputeModule {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+    SummationDensity();
+    void compute() override;
+    void update() { compute(); }
+
+    DEF_EMPTY_VAR(RestDensity, Real, "Rest density");
+    DEF_EMPTY_VAR(SamplingDistance, Real, "Sampling distance");
+    DEF_EMPTY_VAR(SmoothingLength, Real, "Smoothing length");
+    DEF_EMPTY_IN_ARRAY(Position, Coord, DeviceType::GPU, "Particle position");
+    DEF_EMPTY_IN_NEIGHBOR_LIST(NeighborIndex, int, "Neighboring particles");
+    DEF_EMPTY_OUT_ARRAY(Density, Real, DeviceType::GPU, "Particle density");
+};
+
+template <typename TDataType>
+class DensityPBD : public ConstraintModule {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+
+    DensityPBD();
+    ~DensityPBD() override = default;
+
+    bool constrain() override;
+    // Runs one Jacobi sweep on the given list (the reference's takeOneIteration).
+    void takeOneIteration();
+    void updateVelocity();
+
+    DEF_EMPTY_VAR(IterationNumber, int, "Iteration number of the PBD solver");
+    DEF_EMPTY_VAR(RestDensity, Real, "Reference density");
+    DEF_EMPTY_VAR(SamplingDistance, Real, "");
+    DEF_EMPTY_VAR(SmoothingLength, Real, "");
+    DEF_EMPTY_IN_ARRAY(Position, Coord, DeviceType::GPU, "Input particle position");
+    DEF_EMPTY_IN_ARRAY(Velocity, Coord, DeviceType::GPU, "Input particle velocity");
+    DEF_EMPTY_IN_NEIGHBOR_LIST(NeighborIndex, int, "Neighboring particles' ids");
+    DEF_EMPTY_OUT_ARRAY(Position, Coord, DeviceType::GPU, "Output particle position");
+    DEF_EMPTY_OUT_ARRAY(Velocity, Coord, DeviceType::GPU, "Output particle velocity");
+    DEF_EMPTY_OUT_ARRAY(Density, Real, DeviceType::GPU, "Final particle density");
+
+private:
+    pk_pbd_params params(int iterations);
+    DeviceArray<Coord> m_position_old;  // scratch velocity of takeOneIteration
+    DeviceArray<Coord> m_x_old;         // positions at the start of constrain()
+};
+
+template <typename TDataType>
+class ParticleIntegrator : public NumericalIntegrator {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+    ParticleIntegrator() = default;
+    void begin() override;
+    void end() override {}
+    bool integrate() override;
+    bool updateVelocity();
+    bool updatePosition();
+
+    DEF_EMPTY_IN_ARRAY(Position, Coord, DeviceType::GPU, "Position");
+    DEF_EMPTY_IN_ARRAY(Velocity, Coord, DeviceType::GPU, "Velocity");
+    DEF_EMPTY_IN_ARRAY(ForceDensity, Coord, DeviceType::GPU, "Force density");
+
+protected:
+    bool initializeImpl() override { return true; }
+
+private:
+    DeviceArray<Coord> m_prePosition, m_preVelocity;
+};
+
+template <typename TDataType>
+class ElasticityModule : public ConstraintModule {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+
+    ElasticityModule();
+    ~ElasticityModule() override = default;
+
+    bool constrain() override;
+    virtual void solveElasticity();
+    void setMu(Real mu) { m_mu.setValue(mu); }
+    void setLambda(Real lambda) { m_lambda.setValue(lambda); }
+    void setIterationNumber(int num) { m_iterNum.setValue(num); }
+    int getIterationNumber() { return m_iterNum.getValue(); }
+    void resetRestShape();
+    // Stretch-break threshold (no reference counterpart; 0 = never break).
+    void setBreakStretch(Real s) { m_breakStretch = s; }
+
+    DEF_EMPTY_IN_VAR(Horizon, Real, "");
+    DEF_EMPTY_IN_ARRAY(Position, Coord, DeviceType::GPU, "Particle position");
+    DEF_EMPTY_IN_ARRAY(Velocity, Coord, DeviceType::GPU, "Particle velocity");
+    DEF_EMPTY_IN_NEIGHBOR_LIST(Neighborhood, int, "Neighboring particles' ids");
+
+protected:
+    bool initializeImpl() override;
+    virtual void enforceElasticity();
+    // Subclasses set m_bulkCoefs here (the reference initialises it to 1).
+    virtual void computeMaterialStiffness();
+
+    VarField<Real> m_mu{Real(0.05)};
+    VarField<Real> m_lambda{Real(0.1)};
+    DeviceArray<Real> m_bulkCoefs;
+
+private:
+    VarField<int> m_iterNum{10};
+    Real m_breakStretch = 0;
+};
+
+// BoundaryConstraint with a box SDF (BoundaryConstraint.cu:108-117).
+template <typename TDataType>
+class BoundaryConstraint : public ConstraintModule {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+    BoundaryConstraint() = default;
+    bool constrain(DeviceArray<Coord>& position, DeviceArray<Coord>& velocity, Real dt);
+    void setCube(Coord lo, Coord hi, Real distance, bool inverted);
+    Real m_normal_friction = 0.95f;
+    Real m_tangent_friction = 0.0f;
+
+private:
+    bool m_set = false;
+    Coord m_lo, m_hi;
+    Real m_distance = 0.005f;
+    bool m_inverted = true;
+};
+
+// PositionBasedFluidModel::step (PositionBasedFluidModel.cpp:83-101) without
+// the viscosity module: begin, NeighborQuery, integrate, DensityPBD, end.
+template <typename TDataType>
+class PositionBasedFluidModel : public NumericalModel {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+    PositionBasedFluidModel();
+    void step(float dt) override;
+    void setNeighborSizeLimit(int cap) { m_cap = cap; }
+    void setIterationNumber(int it) { m_iterations = it; }
+    void setSamplingDistance(Real d) { m_samplingDistance = d; }
+
+    VarField<Real> m_smoothingLength{Real(0.006)};
+    DeviceArrayField<Coord> m_position{0, "position", "", FieldType::In, nullptr};
+    DeviceArrayField<Coord> m_velocity{0, "velocity", "", FieldType::In, nullptr};
+    DeviceArrayField<Coord> m_forceDensity{0, "force_density", "", FieldType::In, nullptr};
+
+    std::shared_ptr<NeighborQuery<TDataType>> m_nbrQuery;
+    std::shared_ptr<DensityPBD<TDataType>> m_pbdModule;
+    std::shared_ptr<ParticleIntegrator<TDataType>> m_integrator;
+
+protected:
+    bool initializeImpl() override;
+
+private:
+    int m_cap = 0;
+    int m_iterations = 3;
+    Real m_samplingDistance = Real(0.005);
+};
+
+// A particle node holding the current state (ParticleSystem.h currentPosition/...).
+template <typename TDataType>
+class ParticleSystem : public Node {
+public:
+    typedef typename TDataType::Coord Coord;
+    explicit ParticleSystem(std::string name = "default") : Node(std::move(name)) {}
+    void setParticles(const std::vector<Coord>& pos, const std::vector<Coord>& vel);
+    void getParticles(std::vector<Coord>& pos, std::vector<Coord>& vel);
+
+    DEF_EMPTY_CURRENT_ARRAY(Position, Coord, DeviceType::GPU, "Particle position");
+    DEF_EMPTY_CURRENT_ARRAY(Velocity, Coord, DeviceType::GPU, "Particle velocity");
+    DEF_EMPTY_CURRENT_ARRAY(Force, Coord, DeviceType::GPU, "Force on each particle");
+};
+
+// ParticleFluid: a particle system stepped by PositionBasedFluidModel.
+template <typename TDataType>
+class ParticleFluid : public ParticleSystem<TDataType> {
+public:
+    typedef typename TDataType::Real Real;
+    explicit ParticleFluid(std::string name = "fluid");
+    bool initialize() override;
+    void advance(float dt) override;
+    std::shared_ptr<PositionBasedFluidModel<TDataType>> getModel() { return m_model_pbf; }
+
+private:
+    std::shared_ptr<PositionBasedFluidModel<TDataType>> m_model_pbf;
+};
+
+// ParticleElasticBody (ParticleElasticBody.cpp:15-98).
+template <typename TDataType>
+class ParticleElasticBody : public ParticleSystem<TDataType> {
+public:
+    typedef typename TDataType::Real Real;
+    explicit ParticleElasticBody(std::string name = "elastic");
+    bool initialize() override;
+    void advance(float dt) override;
+    std::shared_ptr<ElasticityModule<TDataType>> getElasticitySolver();
+    void setElasticitySolver(std::shared_ptr<ElasticityModule<TDataType>> solver);
+    VarField<Real>* varHorizon() { return &m_horizon; }
+
+private:
+    VarField<Real> m_horizon{Real(0.0085)};
+};
+
+// StaticBoundary::advance (StaticBoundary.cpp:45-59): constrain every
+// particle system with every obstacle, before they advance.
+template <typename TDataType>
+class StaticBoundary : public Node {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+    explicit StaticBoundary(std::string name = "boundary") : Node(std::move(name)) {}
+    void loadCube(Coord lo, Coord hi, Real distance = 0.005f, bool bOutBoundary = false);
+    void addParticleSystem(std::shared_ptr<ParticleSystem<TDataType>> p) { m_systems.push_back(p); }
+    void advance(float dt) override;
+
+private:
+    std::vector<std::shared_ptr<BoundaryConstraint<TDataType>>> m_obstacles;
+    std::vector<std::shared_ptr<ParticleSystem<TDataType>>> m_systems;
+};
+
+}  // namespace PhysIKA

@@ -17,6 +17,7 @@ EXPORTED = [
     "pk_ctx_create", "pk_ctx_destroy", "pk_last_error", "pk_ctx_status", "pk_last_launch_count",
     "pk_ctx_profile", "pk_ctx_profile_read",
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
+    "pk_advect", "pk_update_velocity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
 ]
@@ -75,6 +76,8 @@ def load():
         "pk_summation_density": ([P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
         "pk_pbd_solve": ([P, P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
         "pk_integrate": ([P, P, P, P, I, ctypes.POINTER(F * 3), F, P], I),
+        "pk_advect": ([P, P, P, I, F, P], I),
+        "pk_update_velocity": ([P, P, P, P, I, F, P], I),
         "pk_boundary_set_box": ([P, ctypes.POINTER(F * 3), ctypes.POINTER(F * 3), F, I, P], I),
         "pk_boundary_constrain": ([P, P, P, I, F, F, F, P], I),
         "pk_boundary_jitter": ([P, I, P, P], I),

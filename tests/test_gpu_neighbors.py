@@ -74,10 +74,21 @@ def test_outside_grid_and_coincident(oracle):
 
 
 def test_overfull_cells_capped(oracle):
-    # a compressed cluster: ~300 hits per particle, cap 64 selects among them
+    # a compressed cluster: 400 hits per particle, cap 64 selects among them
     rng = np.random.default_rng(9)
-    x = rng.uniform(0.5, 0.508, size=(600, 3)).astype(np.float32)
+    x = rng.uniform(0.5, 0.508, size=(400, 3)).astype(np.float32)
     assert_same_lists(oracle, x, 0.0125, (0, 0, 0), (1, 1, 1), 64)
+
+
+def test_hit_overflow_is_reported(ctx):
+    # more than 512 particles within the radius of each other: the build
+    # reports PK_ERR_CAPACITY instead of returning a truncated list
+    import pkhot
+    rng = np.random.default_rng(10)
+    x = torch.from_numpy(rng.uniform(0.5, 0.508, size=(600, 3)).astype(np.float32)).cuda()
+    ctx.nq_build(x, 0.0125, (0, 0, 0), (1, 1, 1), 64)
+    assert ctx.status() == pkhot.PK_ERR_CAPACITY
+    assert ctx.status() == pkhot.PK_OK  # the condition is cleared once reported
 
 
 def test_dynamic_list_is_symmetric_at_scale(ctx):

@@ -97,7 +97,9 @@ def test_fused_step_1_and_10(ctx, oracle):
             ctx.check_status()
             assert rel(x.cpu().numpy(), xo) < 1e-4, step
             assert rel(v.cpu().numpy(), vo) < 1e-3, step
-    assert np.all(x.cpu().numpy()[:, 1] > 0.0)
+    # the wall acts at the start of each frame; the solve may leave particles a
+    # hair below it until the next frame (as in the reference)
+    assert np.all(x.cpu().numpy()[:, 1] > -0.5 * sc.spacing)
 
 
 def test_fused_step_equals_module_calls(ctx, oracle):
@@ -128,3 +130,22 @@ def test_argument_errors(ctx):
     with pytest.raises(pkhot.PkError) as e:
         ctx.pd_solve(x, x, 0.01)  # before pd_init on a fresh context
     assert e.value.code in (pkhot.PK_ERR_STATE, pkhot.PK_ERR_ARG)
+
+
+def test_fused_step_after_build_with_other_row_stride(oracle):
+    # a fresh context, then an uncapped build (wide rows), then a capped step
+    sc = scenes.dam_break_small(seed=4, n_side=16)
+    c2 = pkhot.Context(0)
+    c2.nq_build(t(sc.x), sc.radius, sc.lo, sc.hi, 0)
+    x, v = t(sc.x), t(sc.v)
+    prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
+                           pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt), sc.gravity,
+                           boundary=False)
+    c2.pbf_step(x, v, prm)
+    c2.check_status()
+    ri, re = oracle.neighbor_query(sc.x, sc.radius, sc.lo, sc.hi, sc.cap)
+    xo, vo = oracle.integrate(sc.x, sc.v, sc.gravity, sc.dt)
+    f, m = oracle.density_scaling(sc.spacing, sc.radius, 1000.0)
+    xo, vo, _ = oracle.pbd_constrain(xo, vo, ri, re, sc.cap, sc.radius, f * m, 5, sc.dt)
+    assert rel(x.cpu().numpy(), xo) < 1e-5
+    c2.close()
