@@ -228,6 +228,25 @@ int pk_pd_solve(pk_ctx* ctx, float* x, float* v, int n, const pk_pd_params* p,
 int pk_pd_get_rest_shape(pk_ctx* ctx, int* rest_idx, float* rest_pos, float* inv_k,
                          pk_stream stream);
 
+/* ------------------------------------------- DensityPBD without allocation */
+
+/* No counterpart in the reference.  For callers that may not allocate device
+ * memory (a host application that owns the GPU memory budget, or a frame loop
+ * that cannot take the synchronisation of cudaMalloc): the same solve as
+ * pk_pbd_solve on a list that was not built by a context, with no context at
+ * all.  Its scratch is one fixed device array inside the library (4 MiB, held
+ * by every GPU that loads the library until exit), so n may be at most
+ * pk_noalloc_max_particles() (131072); larger n returns PK_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU (different streams, or several host threads)
+ * race on it and must be ordered by the caller.  Nothing is allocated or
+ * freed. */
+int pk_noalloc_max_particles(void);
+int pk_pbd_solve_noalloc(float* x, float* v, int n, const int* index, const int* elements,
+                         int cap, long long total, const pk_pbd_params* p, float* rho_out,
+                         pk_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -178,6 +178,8 @@ int check_list(pk_ctx* c, int n, const int* index, const int* elements, int cap,
 
 namespace pk {
 
+float effective_mass_of(const pk_pbd_params* p) { return effective_mass(p); }
+
 void prof_begin(pk_ctx* c, int kind, cudaStream_t st)
 {
     if (!c->prof) return;

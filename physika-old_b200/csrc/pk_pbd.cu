@@ -321,6 +321,31 @@ int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, co
     return launches + 1;
 }
 
+// The same generic solve with caller-supplied scratch (rho_s, lam: n floats;
+// dpos, xold: 3n floats), for the entry point that allocates nothing.
+int pbd_generic_solve_scratch(float* x, float* v, int n, const int* index, const int* elements,
+                              int cap, long long total, const Spiky& k, float mass, int iterations,
+                              float dt, float* rho_out, float* rho_s, float* lam, float* dpos,
+                              float* xold, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const long long m3 = 3LL * n;
+    const unsigned nb3 = (unsigned)((m3 + 255) / 256);
+    int launches = 0;
+    cudaMemcpyAsync(xold, x, sizeof(float) * (size_t)m3, cudaMemcpyDeviceToDevice, st);
+    float* rho = rho_out != nullptr ? rho_out : rho_s;
+    for (int it = 0; it < iterations; ++it) {
+        k_g_density<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho);
+        k_g_lambda<<<nb, 256, 0, st>>>(x, rho, n, index, elements, cap, total, k, lam, dpos);
+        k_g_disp<<<nb, 256, 0, st>>>(x, lam, n, index, elements, cap, total, k, dpos);
+        k_g_add<<<nb3, 256, 0, st>>>(x, dpos, m3);
+        launches += 4;
+    }
+    k_g_velocity<<<nb3, 256, 0, st>>>(v, x, xold, m3, dt);
+    return launches + 1;
+}
+
 // ------------------------------------------------ integrator and boundary
 
 __global__ void __launch_bounds__(256)

@@ -20,6 +20,7 @@ EXPORTED = [
     "pk_advect", "pk_update_velocity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
+    "pk_noalloc_max_particles", "pk_pbd_solve_noalloc",
 ]
 
 
@@ -86,6 +87,8 @@ def load():
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
         "pk_pd_get_rest_shape": ([P, P, P, P, P], I),
+        "pk_noalloc_max_particles": ([], I),
+        "pk_pbd_solve_noalloc": ([P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
