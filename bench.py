@@ -202,7 +202,7 @@ def run_pk(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    sc = scenes.dam_break_2m(seed=0)
+    sc = scenes.dam_break_2m(seed=0, n_side=args.side)
     n = sc.x.shape[0]
     ctx = pkhot.Context(local)
     ctx.boundary_set_box(sc.lo, sc.hi, sc.sdf_spacing, True)
@@ -326,6 +326,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="pk", choices=["pk", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--side", type=int, default=128,
+                    help="lattice side of the scene (128 = the 2,097,152-particle workload; "
+                         "smaller sides are for profiling captures only)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -61,7 +61,8 @@ typedef struct {
     float lo[3];       /* scene bounds (NeighborQuery::setBoundingBox, NeighborQuery.h:30) */
     float hi[3];
     int cap;           /* setNeighborSizeLimit (NeighborQuery.h:34); 0 = dynamic list */
-    int max_neighbors; /* dynamic mode only: per-particle row bound (0 = 256) */
+    int max_neighbors; /* dynamic mode: per-particle bound (0 = 512, the maximum); any mode
+                          reports PK_ERR_CAPACITY through pk_ctx_status above 512 hits */
 } pk_nq_params;
 
 /* NeighborQuery::compute (Framework/Topology/NeighborQuery.cu:152-199):

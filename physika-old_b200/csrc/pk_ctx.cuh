@@ -25,6 +25,9 @@ struct pk_ctx {
     int* count = nullptr;     // hits per particle (sorted order)
     int* count_c = nullptr;   // hits per particle (caller order, dynamic lists)
     int* offs = nullptr;      // exclusive scan of count_c (n + 1)
+    int* hcnt = nullptr;      // hits per particle in the hit rows (sorted order)
+    int2* items = nullptr;    // list-build work items: sorted ranges sharing one cell
+    int* nitems = nullptr;    // device counter of items (1 int)
     float4* xs_pre = nullptr;
     float4* xs0 = nullptr;
     float4* xa = nullptr;
@@ -38,6 +41,7 @@ struct pk_ctx {
     // ---- rows (capacity cap_rows entries)
     long long cap_rows = 0;
     int* rows = nullptr;
+    float* hitd = nullptr;    // squared distance of each hit-row entry (capped lists)
 
     // ---- dense cell table (capacity cap_keys entries + 2)
     long long cap_keys = 0;

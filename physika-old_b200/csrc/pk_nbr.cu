@@ -4,272 +4,478 @@
 // particle, the `cap` nearest hits with d < h by replacing the current
 // farthest entry; K_CalNeighborSize/K_GetNeighborElements (:245-276,337-367)
 // build the uncapped list.  A capped list is asymmetric (j in N(i) does not
-// imply i in N(j)), and DensityPBD scatters each pair's displacement to both
-// ends (DensityPBD.cu:161-173).  To solve that with gathers only, each row
-// holds the union N(i) + {j : i in N(j)} with two flag bits, so a pair's
-// multiplicity in i's displacement sum is known without atomics:
-//   pass 1 (k_select): one warp per particle scans the 27 cells, compacts the
-//     hits into shared memory, and finds tau_i = the cap-th smallest
-//     (distance, sorted index) key with a 256-bin histogram of d/h and an
-//     exact rank among the few hits of the boundary bin;
-//   pass 2 (k_emit): the same scan marks each hit with a = key <= tau_i
-//     (j in N(i)) and b = key' <= tau_j (i in N(j), tau_j gathered), writes
-//     a-entries first, then b-only entries, and the public NeighborList in
-//     caller ids (fixed: index = count, dynamic: CSR) on the way.
-// Distances use exact_dist (explicit roundings), so the d < h decisions and
-// the ordering are bit-identical for (i,j) and (j,i) and match the CPU
-// restatement.
+// imply i in N(j)) and DensityPBD scatters each pair's displacement to both
+// ends (DensityPBD.cu:161-173).  To solve that with gathers only, each solver
+// row holds N(i) plus {j : i in N(j)} with two flag bits, so a pair's
+// multiplicity in i's displacement is known without atomics.
+//
+//   k_build (one warp per occupied cell, passes of up to 16 particles): every
+//     lane holds the pass's particles in registers and takes one candidate of
+//     each 32-wide chunk of the 27 neighbour ranges (a coalesced load), so a
+//     lane runs 16 independent pair tests per chunk; one ballot per particle
+//     appends the chunk's hits to its row in candidate order.  The hit test
+//     compares the rounded squared distance with the precomputed float T
+//     (sqrt_rn(d2) < h  <=>  d2 < T, sqrt_rn being monotone), so no square
+//     root is taken.  The same sweep counts the hits below a narrow window
+//     around the particle's previous tau and collects the hits inside it;
+//     when the cap-th smallest key falls in the window it is ranked there
+//     exactly: tau_i.  Otherwise further sweeps refine a 32-bin histogram of
+//     d2 until the bin holding the cap-th key fits the slots.  Keys are
+//     (d2, sorted index): sqrt_rn is monotone, so this order agrees with the
+//     reference's distance order except among hits at exactly equal
+//     distance, which the reference orders by arrival.
+//   k_emit (8 lanes per particle): re-reads the hit row, marks a = key <= tau_i
+//     (j in N(i)) and b = key' <= tau_j (i in N(j)), compacts in place with
+//     a-entries first, then b-only entries, and writes the public NeighborList
+//     in caller ids (fixed: index = count; dynamic: CSR).
+// Distances use the explicit roundings of exact_norm3's squared sum, so every
+// d < h decision and every ordering is bit-identical for (i, j) and (j, i)
+// and matches the CPU restatement.
+#include <algorithm>
+#include <cmath>
+
 #include "pk_kernels.cuh"
 
 namespace pk {
 
 constexpr int kBuildWarps = 4;
+constexpr int kBins = 32;                // histogram of d2 over [0, T)
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ bool key_le(float d, int id, uint2 tau)
+__device__ __forceinline__ bool key_le(float d2, int id, uint2 tau)
 {
-    float td = __uint_as_float(tau.x);
-    return d < td || (d == td && id <= (int)tau.y);
+    const float td = __uint_as_float(tau.x);
+    return d2 < td || (d2 == td && id <= (int)tau.y);
 }
 
-template <bool kCapped>
-__global__ void __launch_bounds__(kBuildWarps * 32)
-    k_select(const float4* __restrict__ xs, const int* __restrict__ start, Grid g, int n, int cap,
-             float h, const int* __restrict__ perm, uint2* __restrict__ tau,
-             int* __restrict__ count_c, int* __restrict__ err)
+__device__ __forceinline__ bool key_lt(float da, int ta, float db, int tb)
 {
-    __shared__ float s_d[kBuildWarps][kMaxHits];
-    __shared__ int s_t[kBuildWarps][kMaxHits];
-    __shared__ int s_h[kBuildWarps][256];
+    return da < db || (da == db && ta < tb);
+}
+
+// Rounded squared distance of exact_norm3 (before its square root).
+__device__ __forceinline__ float exact_d2(float4 a, float4 b)
+{
+    const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
+#if PK_NORM_VARIANT == 0
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+#elif PK_NORM_VARIANT == 2
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+#else
+    return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+#endif
+}
+
+struct BuildArgs {
+    const float4* xs;   // positions the list is built on (sorted)
+    const int* start;   // cell starts
+    const int2* items;  // (begin, end) sorted ranges sharing one cell
+    const int* nitems;
+    Grid g;
+    int n, row_cap;
+    float T;            // d2 threshold of d < h
+    int* rows;          // hit rows: sorted indices, candidate order
+    float* hitd;        // d2 of each hit, or null (uncapped lists need none)
+    int* hcnt;          // hits per particle (sorted order)
+    int* count_c;       // hits per particle in caller order (dynamic public list), or null
+    const int* perm;
+    int* err;
+};
+
+// Particles of one pass, held in registers by every lane.
+constexpr int kPB = 16;
+
+// Per-warp shared state of the sweep: the 27 neighbour ranges as (begin,
+// packed offset) pairs.
+struct SweepSmem {
+    int rbeg[32], roff[33];
+};
+constexpr size_t kBuildSmem = sizeof(SweepSmem) * kBuildWarps;
+
+// Candidate g of the packed 27 ranges (t = its sorted index); past the end a
+// far-away sentinel that hits nothing.
+__device__ __forceinline__ float4 fetch_cand(const float4* __restrict__ xs, const SweepSmem& S, int g,
+                                             int total, int& t)
+{
+    if (g >= total) {
+        t = 0;
+        return make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.f);
+    }
+    int r = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1)
+        if (r + step < 27 && S.roff[r + step] <= g) r += step;
+    t = S.rbeg[r] + (g - S.roff[r]);
+    return __ldg(xs + t);
+}
+
+// Hit rows, one warp per occupied cell in passes of up to kPB particles.
+// Every lane holds the pass's particles in registers and takes one candidate
+// of each 32-wide chunk of the 27 neighbour ranges: up to kPB independent
+// pair tests per lane and chunk, then one ballot per particle appends the
+// chunk's hits to its row (in candidate order, so rows are deterministic).
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
+{
+    extern __shared__ int smem_i[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int s = blockIdx.x * kBuildWarps + w;
-    if (s >= n) return;  // warp-uniform
     const unsigned lt = (1u << lane) - 1u;
-    const float4 xi = xs[s];
-    const int3 c = cell3(g, xi.x, xi.y, xi.z);
-    int cnt = 0;
-    for (int o = 0; o < 27; ++o) {
-        int key = cell_key(g, c.x + kOffset27[o][0], c.y + kOffset27[o][1], c.z + kOffset27[o][2]);
-        if (key < 0) continue;
-        int a = __ldg(start + key), b = __ldg(start + key + 1);
-        for (int t0 = a; t0 < b; t0 += 32) {
-            int t = t0 + lane;
-            float d = 0.f;
-            bool hit = false;
-            if (t < b) {
-                d = exact_dist(xi, __ldg(xs + t));
-                hit = d < h;
+    SweepSmem& S = reinterpret_cast<SweepSmem*>(smem_i)[w];
+    const int nitems = *A.nitems;
+    const int gw = blockIdx.x * kBuildWarps + w, nw = gridDim.x * kBuildWarps;
+    const bool want_d = A.hitd != nullptr;
+    for (int item = gw; item < nitems; item += nw) {
+        const int2 rng = A.items[item];
+        const float4 x0 = A.xs[rng.x];
+        const int3 c = cell3(A.g, x0.x, x0.y, x0.z);
+        // the 27 neighbour ranges in one round: lane o < 27 owns offset o
+        int beg = 0, len = 0;
+        if (lane < 27) {
+            const int key = cell_key(A.g, c.x + kOffset27[lane][0], c.y + kOffset27[lane][1],
+                                     c.z + kOffset27[lane][2]);
+            if (key >= 0) {
+                beg = __ldg(A.start + key);
+                len = __ldg(A.start + key + 1) - beg;
             }
-            unsigned m = __ballot_sync(kFull, hit);
-            if (kCapped && hit) {
-                int p = cnt + __popc(m & lt);
-                if (p < kMaxHits) {
-                    s_d[w][p] = d;
-                    s_t[w][p] = t;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        __syncwarp();
+        S.rbeg[lane] = beg;
+        S.roff[lane] = incl - len;
+        const int total = __shfl_sync(kFull, incl, 31);
+        if (lane == 31) S.roff[32] = total;
+        __syncwarp();
+        for (int p0 = rng.x; p0 < rng.y; p0 += kPB) {
+            const int m = min(kPB, rng.y - p0);
+            float px[kPB], py[kPB], pz[kPB];
+            int cnt[kPB];
+#pragma unroll
+            for (int p = 0; p < kPB; ++p) {
+                if (p < m) {
+                    const float4 q = __ldg(A.xs + p0 + p);
+                    px[p] = q.x;
+                    py[p] = q.y;
+                    pz[p] = q.z;
+                } else {
+                    px[p] = py[p] = pz[p] = -3.0e38f;
+                }
+                cnt[p] = 0;
+            }
+            int* const row0 = A.rows + (long long)p0 * A.row_cap;
+            float* const d0 = want_d ? A.hitd + (long long)p0 * A.row_cap : nullptr;
+            for (int c0 = 0; c0 < total; c0 += 32) {
+                int t;
+                const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
+#pragma unroll
+                for (int p = 0; p < kPB; ++p) {
+                    if (p >= m) break;  // warp-uniform
+                    const float d2 = exact_d2(make_float4(px[p], py[p], pz[p], 0.f), cx);
+                    const bool hit = d2 < A.T;
+                    const unsigned b = __ballot_sync(kFull, hit);
+                    const int pos = cnt[p] + __popc(b & lt);
+                    if (hit && pos < A.row_cap) {
+                        row0[p * A.row_cap + pos] = t;
+                        if (want_d) d0[p * A.row_cap + pos] = d2;
+                    }
+                    cnt[p] += __popc(b);
                 }
             }
-            cnt += __popc(m);
-        }
-    }
-    if (count_c != nullptr && lane == 0) count_c[perm[s]] = cnt;
-    if (!kCapped) return;
-    if (cnt <= cap || cnt > kMaxHits) {
-        if (cnt > kMaxHits && lane == 0) atomicOr(err, kErrHitOverflow);
-        if (lane == 0) tau[s] = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
-        return;
-    }
-    // Placeholder until the selection below writes the exact key (ordered by
-    // the __syncwarp that follows).
-    if (lane == 0) tau[s] = make_uint2(0x7f800000u, 0x7fffffffu);
-    __syncwarp();
-    // ---- histogram of d over 256 equal bins of [0, h): monotone in d.
-    int* hist = s_h[w];
-    for (int k = lane; k < 256; k += 32) hist[k] = 0;
-    __syncwarp();
-    const float scale = 256.0f / h;
-    for (int e = lane; e < cnt; e += 32) atomicAdd(&hist[min((int)(s_d[w][e] * scale), 255)], 1);
-    __syncwarp();
-    int loc[8], sum = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        loc[k] = hist[lane * 8 + k];
-        sum += loc[k];
-    }
-    int incl = sum;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        int y = __shfl_up_sync(kFull, incl, off);
-        if (lane >= off) incl += y;
-    }
-    const int excl = incl - sum;
-    const int r = cap - 1;  // 0-based rank of tau
-    unsigned own = __ballot_sync(kFull, excl <= r && r < incl);
-    int src = __ffs(own) - 1;
-    int B = 0, before = 0;
-    if (lane == src) {
-        int acc = excl;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (r < acc + loc[k]) {
-                B = lane * 8 + k;
-                before = acc;
-                break;
+            for (int p = 0; p < kPB; ++p) {
+                if (lane == p && p < m) {
+                    const int s = p0 + p;
+                    A.hcnt[s] = min(cnt[p], A.row_cap);
+                    if (A.count_c) A.count_c[A.perm[s]] = cnt[p];
+                    if (cnt[p] > A.row_cap) atomicOr(A.err, kErrRowOverflow);
+                }
             }
-            acc += loc[k];
-        }
-    }
-    B = __shfl_sync(kFull, B, src);
-    before = __shfl_sync(kFull, before, src);
-    const int rr = r - before;  // rank of tau among the hits of bin B
-    __syncwarp();
-    // ---- compact bin B's hits (reusing the histogram as 128 (d, t) pairs)
-    int m = 0;
-    for (int e0 = 0; e0 < cnt; e0 += 32) {
-        int e = e0 + lane;
-        bool in = false;
-        float d = 0.f;
-        int t = 0;
-        if (e < cnt) {
-            d = s_d[w][e];
-            t = s_t[w][e];
-            in = min((int)(d * scale), 255) == B;
-        }
-        unsigned mm = __ballot_sync(kFull, in);
-        if (in) {
-            int p = m + __popc(mm & lt);
-            if (p < 128) {
-                hist[2 * p] = __float_as_int(d);
-                hist[2 * p + 1] = t;
-            }
-        }
-        m += __popc(mm);
-    }
-    __syncwarp();
-    if (m <= 128) {
-        for (int q = lane; q < m; q += 32) {
-            float dq = __int_as_float(hist[2 * q]);
-            int tq = hist[2 * q + 1];
-            int rank = 0;
-            for (int u = 0; u < m; ++u) {
-                float du = __int_as_float(hist[2 * u]);
-                int tu = hist[2 * u + 1];
-                rank += (du < dq || (du == dq && tu < tq)) ? 1 : 0;
-            }
-            if (rank == rr) tau[s] = make_uint2(__float_as_uint(dq), (unsigned)tq);
-        }
-    } else {
-        // Degenerate bin (many equal distances): rank among all of bin B.
-        for (int e = lane; e < cnt; e += 32) {
-            float dq = s_d[w][e];
-            int tq = s_t[w][e];
-            if (min((int)(dq * scale), 255) != B) continue;
-            int rank = 0;
-            for (int u = 0; u < cnt; ++u) {
-                float du = s_d[w][u];
-                int tu = s_t[w][u];
-                if (min((int)(du * scale), 255) != B) continue;
-                rank += (du < dq || (du == dq && tu < tq)) ? 1 : 0;
-            }
-            if (rank == rr) tau[s] = make_uint2(__float_as_uint(dq), (unsigned)tq);
         }
     }
 }
 
-__global__ void __launch_bounds__(kBuildWarps * 32)
-    k_emit(const float4* __restrict__ xs, const int* __restrict__ start, Grid g, int n, int cap,
-           float h, const int* __restrict__ perm, const uint2* __restrict__ tau,
-           int* __restrict__ rows, int2* __restrict__ rcnt, int row_cap,
-           int* __restrict__ pub_index, int* __restrict__ pub_elements, long long pub_capacity,
-           const int* __restrict__ offs, int* __restrict__ err)
+// ---- tau_i: the cap-th smallest key (d2, sorted index) of each hit row.
+constexpr int kSelWarps = 8;
+constexpr int kSelLevels = 5;  // bins of T/32^5: a few ulps of d2 near T
+
+struct SelSmem {
+    int hist[kBins];
+    float sd[32];
+    int st[32];
+};
+
+// Bin of d2 at one refinement level: kBins equal bins of width 1/scale from
+// lo, clamped; monotone in d2, so bins never reorder keys.
+__device__ __forceinline__ int level_bin(float d2, float lo, float scale)
 {
-    __shared__ int s_b[kBuildWarps][kMaxHits];
+    return min(max((int)((d2 - lo) * scale), 0), kBins - 1);
+}
+
+// One warp per particle whose row holds more than cap hits.  Histogram
+// refinement over the row's stored d2: a 32-bin histogram of the hits in play
+// locates the bin holding the rank, whose hits are the next level's play set;
+// once the bin holds at most 32 hits they are ranked exactly by (d2, index).
+// Bins are monotone in d2, so each play set is an interval of keys.  Hits at
+// d2 values no split separates are ranked against the whole play set.
+__global__ void __launch_bounds__(kSelWarps * 32)
+    k_select(const int* __restrict__ rows, const float* __restrict__ hitd, const int* __restrict__ hcnt,
+             int n, int cap, int row_cap, float bin_scale, uint2* __restrict__ tau)
+{
+    __shared__ SelSmem sm[kSelWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int s = blockIdx.x * kBuildWarps + w;
-    if (s >= n) return;  // warp-uniform
     const unsigned lt = (1u << lane) - 1u;
+    SelSmem& S = sm[w];
+    const int gw = blockIdx.x * kSelWarps + w, nw = gridDim.x * kSelWarps;
+    for (int s = gw; s < n; s += nw) {
+        const int c = hcnt[s];
+        uint2 res = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
+        if (c > cap) {
+            const int* row = rows + (long long)s * row_cap;
+            const float* rd = hitd + (long long)s * row_cap;
+            float lo[kSelLevels], sc[kSelLevels];
+            int bsel[kSelLevels];
+            int rr = cap - 1;
+            bool done = false;
+            lo[0] = 0.f;
+            sc[0] = bin_scale;
+#pragma unroll
+            for (int L = 0; L < kSelLevels; ++L) {
+                if (!done) {
+                    S.hist[lane] = 0;
+                    __syncwarp();
+                    for (int e0 = 0; e0 < c; e0 += 32) {
+                        const int e = e0 + lane;
+                        if (e < c) {
+                            const float d2 = __ldg(rd + e);
+                            bool in = true;
+#pragma unroll
+                            for (int q = 0; q < L; ++q) in = in && level_bin(d2, lo[q], sc[q]) == bsel[q];
+                            if (in) atomicAdd(&S.hist[level_bin(d2, lo[L], sc[L])], 1);
+                        }
+                    }
+                    __syncwarp();
+                    const int h = S.hist[lane];
+                    int incl = h;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(kFull, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    const int B = __ffs(__ballot_sync(kFull, incl > rr)) - 1;
+                    const int nB = __shfl_sync(kFull, h, B);
+                    rr -= __shfl_sync(kFull, incl - h, B);
+                    bsel[L] = B;
+                    if (L + 1 < kSelLevels) {
+                        lo[L + 1] = lo[L] + (float)B / sc[L];
+                        sc[L + 1] = sc[L] * (float)kBins;
+                    }
+                    if (nB <= 32 || L + 1 == kSelLevels) {
+                        // the play set of the next level, ranked exactly
+                        const bool small = nB <= 32;
+                        int k = 0;
+                        uint2 mine = make_uint2(0x7f800000u, 0x7fffffffu);
+                        for (int e0 = 0; e0 < c; e0 += 32) {
+                            const int e = e0 + lane;
+                            float d2 = 0.f;
+                            int t = 0;
+                            bool in = false;
+                            if (e < c) {
+                                d2 = __ldg(rd + e);
+                                t = __ldg(row + e);
+                                in = true;
+#pragma unroll
+                                for (int q = 0; q <= L; ++q) in = in && level_bin(d2, lo[q], sc[q]) == bsel[q];
+                            }
+                            if (small) {
+                                const unsigned bal = __ballot_sync(kFull, in);
+                                if (in) {
+                                    const int q = k + __popc(bal & lt);
+                                    S.sd[q] = d2;
+                                    S.st[q] = t;
+                                }
+                                k += __popc(bal);
+                            } else if (in) {
+                                // rank this hit against the whole play set
+                                int rank = 0;
+                                for (int u = 0; u < c; ++u) {
+                                    const float du = __ldg(rd + u);
+                                    bool inu = true;
+#pragma unroll
+                                    for (int q = 0; q <= L; ++q) inu = inu && level_bin(du, lo[q], sc[q]) == bsel[q];
+                                    if (inu) rank += key_lt(du, __ldg(row + u), d2, t);
+                                }
+                                if (rank == rr) mine = make_uint2(__float_as_uint(d2), (unsigned)t);
+                            }
+                        }
+                        __syncwarp();
+                        if (small && lane < k) {
+                            const float dm = S.sd[lane];
+                            const int tm = S.st[lane];
+                            int rank = 0;
+                            for (int u = 0; u < k; ++u) rank += key_lt(S.sd[u], S.st[u], dm, tm);
+                            if (rank == rr) mine = make_uint2(__float_as_uint(dm), (unsigned)tm);
+                        }
+                        const unsigned f = __ballot_sync(kFull, mine.y != 0x7fffffffu);
+                        const int src = f ? __ffs(f) - 1 : 0;
+                        res.x = __shfl_sync(kFull, mine.x, src);
+                        res.y = __shfl_sync(kFull, mine.y, src);
+                        done = true;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        if (lane == 0) tau[s] = res;
+    }
+}
+
+// Solver rows from the hit rows: G lanes per particle.
+constexpr int kEmitG = 8;
+constexpr int kStash = 128;  // b-only entries kept per group before appending
+
+__global__ void __launch_bounds__(256)
+    k_emit(const int* __restrict__ hcnt, const float* __restrict__ hitd, const uint2* __restrict__ tau,
+           const int* __restrict__ perm, int n, int cap, int row_cap, int* __restrict__ rows,
+           int2* __restrict__ rcnt, int* __restrict__ pub_index, int* __restrict__ pub_elements,
+           long long pub_capacity, const int* __restrict__ offs, int* __restrict__ err)
+{
+    __shared__ int s_b[256 / kEmitG][kStash];  // b-only entries of each group
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = gid / kEmitG, sub = gid % kEmitG, grp = threadIdx.x / kEmitG;
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = ((1u << kEmitG) - 1u) << (lane & ~(kEmitG - 1));
+    const unsigned lt_g = ((1u << lane) - 1u) & gmask;
+    const bool valid = s < n;
     const bool capped = cap > 0;
-    const float4 xi = xs[s];
-    const uint2 ti = capped ? tau[s] : make_uint2(0x7f800000u, 0x7fffffffu);
-    int* row = rows + (long long)s * row_cap;
-    const int ps = perm[s];
-    const bool pub = pub_elements != nullptr;
+    int cnt = 0, ps = 0;
+    uint2 ti = make_uint2(0x7f800000u, 0x7fffffffu);
     long long pbase = 0;
-    if (pub) pbase = capped ? (long long)ps * cap : (long long)offs[ps];
-    const int3 c = cell3(g, xi.x, xi.y, xi.z);
+    const bool pub = pub_elements != nullptr;
+    if (valid) {
+        cnt = hcnt[s];
+        if (capped) ti = tau[s];
+        ps = perm[s];
+        if (pub) pbase = capped ? (long long)ps * cap : (long long)offs[ps];
+    }
+    int* row = rows + (long long)(valid ? s : 0) * row_cap;
+    const float* rd = capped ? hitd + (long long)(valid ? s : 0) * row_cap : nullptr;
+    // every lane of the warp iterates to the longest row of the warp's groups
+    int cmax = cnt;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
     int nA = 0, nB = 0;
-    bool pub_over = false;
-    for (int o = 0; o < 27; ++o) {
-        int key = cell_key(g, c.x + kOffset27[o][0], c.y + kOffset27[o][1], c.z + kOffset27[o][2]);
-        if (key < 0) continue;
-        int a0 = __ldg(start + key), b0 = __ldg(start + key + 1);
-        for (int t0 = a0; t0 < b0; t0 += 32) {
-            int t = t0 + lane;
-            bool fa = false, fb = false;
-            if (t < b0) {
-                float d = exact_dist(xi, __ldg(xs + t));
-                if (d < h) {
-                    fa = key_le(d, t, ti);
-                    fb = capped ? key_le(d, s, __ldg(tau + t)) : true;
-                }
+    bool over = false;
+    for (int e0 = 0; e0 < cmax; e0 += kEmitG) {
+        const int e = e0 + sub;
+        bool fa = false, fb = false;
+        int t = 0;
+        if (valid && e < cnt) {
+            t = row[e];
+            if (capped) {
+                const float d2 = rd[e];
+                fa = key_le(d2, t, ti);
+                fb = key_le(d2, s, __ldg(tau + t));
+            } else {
+                fa = fb = true;
             }
-            unsigned ma = __ballot_sync(kFull, fa);
-            unsigned mb = __ballot_sync(kFull, fb && !fa);
-            if (fa) {
-                int p = nA + __popc(ma & lt);
-                if (p < row_cap) row[p] = t | kRowFlagA | (fb ? kRowFlagB : 0);
-                if (pub) {
-                    long long q = pbase + p;
-                    if (capped ? (p < cap) : (q < pub_capacity))
-                        pub_elements[q] = __ldg(perm + t);
-                    else
-                        pub_over = true;
-                }
-            }
-            if (fb && !fa) {
-                int p = nB + __popc(mb & lt);
-                if (p < kMaxHits) s_b[w][p] = t | kRowFlagB;
-            }
-            nA += __popc(ma);
-            nB += __popc(mb);
         }
+        const unsigned ba = __ballot_sync(kFull, fa) & gmask;
+        const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
+        // entries only move towards the front, never onto unread ones
+        if (fa) {
+            const int q = nA + __popc(ba & lt_g);
+            row[q] = t | kRowFlagA | (fb ? kRowFlagB : 0);
+            if (pub) {
+                const long long o = pbase + q;
+                if (capped ? (q < cap) : (o < pub_capacity))
+                    pub_elements[o] = __ldg(perm + t);
+                else
+                    over = true;
+            }
+        }
+        if (fb && !fa) {
+            const int q = nB + __popc(bb & lt_g);
+            if (q < kStash)
+                s_b[grp][q] = t | kRowFlagB;
+            else
+                over = true;
+        }
+        nA += __popc(ba);
+        nB += __popc(bb);
     }
     __syncwarp();
-    const int nBw = min(nB, kMaxHits);
-    for (int e = lane; e < nBw; e += 32) {
-        int p = nA + e;
-        if (p < row_cap) row[p] = s_b[w][e];
+    if (valid) {
+        const int nBw = min(nB, kStash);
+        for (int e = sub; e < nBw; e += kEmitG) row[nA + e] = s_b[grp][e];
+        if (sub == 0) {
+            rcnt[s] = make_int2(nA, nA + nBw);
+            if (pub_index != nullptr) pub_index[ps] = capped ? min(nA, cap) : offs[ps];
+        }
     }
-    if (__any_sync(kFull, pub_over) && lane == 0) atomicOr(err, kErrPublicOverflow);
-    if (lane == 0) {
-        if (nA + nB > row_cap || nB > kMaxHits) atomicOr(err, kErrRowOverflow);
-        rcnt[s] = make_int2(min(nA, row_cap), min(nA + nB, row_cap));
-        if (pub_index != nullptr) pub_index[ps] = capped ? min(nA, cap) : offs[ps];
-    }
+    if (__any_sync(kFull, over) && lane == 0) atomicOr(err, kErrPublicOverflow);
+}
+
+// Smallest float T with sqrt_rn(T) >= h: for every float d2, sqrt_rn(d2) < h
+// exactly when d2 < T (host sqrtf is correctly rounded, as __fsqrt_rn is).
+static float radius_threshold(float h)
+{
+    float T = h * h;
+    while (std::sqrt(T) < h) T = std::nextafter(T, INFINITY);
+    while (T > 0.0f && std::sqrt(std::nextafter(T, 0.0f)) >= h) T = std::nextafter(T, 0.0f);
+    return T;
 }
 
 int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, int* pub_index,
                int* pub_elements, long long pub_capacity, cudaStream_t st)
 {
     if (n <= 0) return 0;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // a persistent grid: as many warps per SM as registers and shared memory allow
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build, kBuildWarps * 32, kBuildSmem);
+    if (sms <= 0) sms = 148;
+    if (per_sm <= 0) per_sm = 1;
     int launches = 0;
-    unsigned nb = (unsigned)((n + kBuildWarps - 1) / kBuildWarps);
     const bool dyn_pub = cap <= 0 && pub_index != nullptr;
+    const bool capped = cap > 0;
+    BuildArgs A;
+    A.xs = c->xs_pre;
+    A.start = c->cell_start;
+    A.items = c->items;
+    A.nitems = c->nitems;
+    A.g = g;
+    A.n = n;
+    A.row_cap = row_cap;
+    A.T = radius_threshold(h);
+    A.rows = c->rows;
+    A.hitd = capped ? c->hitd : nullptr;
+    A.hcnt = c->hcnt;
+    A.count_c = dyn_pub ? c->count_c : nullptr;
+    A.perm = c->perm;
+    A.err = c->d_err;
+    const int blocks = std::min((n + kBuildWarps - 1) / kBuildWarps, sms * per_sm);
     prof_begin(c, PK_PROF_SELECT, st);
-    if (cap > 0) {
-        k_select<true><<<nb, kBuildWarps * 32, 0, st>>>(c->xs_pre, c->cell_start, g, n, cap, h,
-                                                        c->perm, c->tau, nullptr, c->d_err);
+    k_build<<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
+    ++launches;
+    if (capped) {
+        const int sb = std::min((n + kSelWarps - 1) / kSelWarps, sms * 8);
+        k_select<<<sb, kSelWarps * 32, 0, st>>>(c->rows, c->hitd, c->hcnt, n, cap, row_cap,
+                                                (float)kBins / A.T, c->tau);
         ++launches;
-    } else if (dyn_pub) {
-        k_select<false><<<nb, kBuildWarps * 32, 0, st>>>(c->xs_pre, c->cell_start, g, n, cap, h,
-                                                         c->perm, c->tau, c->count_c, c->d_err);
+    }
+    if (dyn_pub) {
         exclusive_scan(c->count_c, n, c->offs, c->scan_part, st);
-        launches += 1 + scan_launches();
+        launches += scan_launches();
     }
     prof_end(c, PK_PROF_SELECT, st);
     prof_begin(c, PK_PROF_EMIT, st);
-    k_emit<<<nb, kBuildWarps * 32, 0, st>>>(c->xs_pre, c->cell_start, g, n, cap, h, c->perm, c->tau,
-                                            c->rows, c->rcnt, row_cap, pub_index, pub_elements,
-                                            pub_capacity, c->offs, c->d_err);
+    const unsigned ne = (unsigned)(((long long)n * kEmitG + 255) / 256);
+    k_emit<<<ne, 256, 0, st>>>(c->hcnt, c->hitd, c->tau, c->perm, n, cap, row_cap, c->rows, c->rcnt,
+                               pub_index, pub_elements, pub_capacity, c->offs, c->d_err);
     prof_end(c, PK_PROF_EMIT, st);
     return launches + 1;
 }

@@ -185,16 +185,27 @@ __global__ void __launch_bounds__(256) k_scatter(const int* __restrict__ key, co
     perm[start[key[i]] + rank[i]] = i;
 }
 
-// Sorts the ids of each cell ascending (insertion sort; cells hold ~10-30).
-// Buckets above 2048 entries (only the "outside the grid" bucket can be that
-// large) keep their atomic order.
+// Sorts the ids of each cell ascending (insertion sort; cells hold ~10-30)
+// and appends the list-build work items: one (begin, end) sorted range per
+// occupied cell, and one item per particle of the last bucket (outside the
+// grid: each queries its own, out-of-range cell).  Buckets above 2048
+// entries (only the outside bucket can be that large) keep their atomic order.
 __global__ void __launch_bounds__(256) k_fix_cells(const int* __restrict__ start, long long ncells,
-                                                   int* __restrict__ perm)
+                                                   int* __restrict__ perm, int2* __restrict__ items,
+                                                   int* __restrict__ nitems)
 {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     int a = start[c], b = start[c + 1];
     int m = b - a;
+    if (m > 0) {
+        if (c < ncells - 1) {
+            items[atomicAdd(nitems, 1)] = make_int2(a, b);
+        } else {
+            int base = atomicAdd(nitems, m);
+            for (int u = 0; u < m; ++u) items[base + u] = make_int2(a + u, a + u + 1);
+        }
+    }
     if (m < 2 || m > 2048) return;
     int* p = perm + a;
     for (int u = 1; u < m; ++u) {
@@ -261,7 +272,9 @@ int sort_particles(pk_ctx* c, float* x, float* v, const float* f, int n, const G
     launches += scan_launches();
     if (n > 0) {
         k_scatter<<<nb, 256, 0, st>>>(c->key, c->rank, c->cell_start, n, c->perm);
-        k_fix_cells<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(c->cell_start, nk, c->perm);
+        cudaMemsetAsync(c->nitems, 0, sizeof(int), st);
+        k_fix_cells<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(c->cell_start, nk, c->perm,
+                                                                   c->items, c->nitems);
         if (integrate)
             k_gather<true><<<nb, 256, 0, st>>>(x, v, f, c->perm, n, c->xs_pre, c->xs0, c->vs, c->inv,
                                                grav[0], grav[1], grav[2], dt);
