@@ -53,7 +53,7 @@ int ensure_particles(pk_ctx* c, int n)
     bool ok = regrow(c->perm, m) && regrow(c->inv, m) && regrow(c->key, m) && regrow(c->rank, m) &&
               regrow(c->count, m) && regrow(c->count_c, m) && regrow(c->offs, m + 1) &&
               regrow(c->xs_pre, m) && regrow(c->xs0, m) && regrow(c->xa, m) && regrow(c->xb, m) &&
-              regrow(c->vs, m) && regrow(c->lam, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
+              regrow(c->vs, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
               regrow(c->tau, m) && regrow(c->hcnt, m) && regrow(c->items, m + 1) &&
               regrow(c->nitems, 1);
     if (!ok) {
@@ -67,7 +67,7 @@ int ensure_particles(pk_ctx* c, int n)
 int ensure_rows(pk_ctx* c, long long m)
 {
     if (m <= c->cap_rows) return PK_OK;
-    if (!regrow(c->rows, (size_t)m) || !regrow(c->hitd, (size_t)m)) {
+    if (!regrow(c->rows, (size_t)m) || !regrow(c->hits, (size_t)m)) {
         c->cap_rows = 0;
         return fail(c, PK_ERR_NOMEM, "device allocation of neighbour rows failed");
     }
@@ -238,9 +238,9 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
     void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
-                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->lam, c->rho, c->rcnt, c->tau,
+                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->rho, c->rcnt, c->tau,
                     c->hcnt, c->items, c->nitems,
-                    c->rows, c->hitd, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
+                    c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w};
     for (void* p : ptrs)

@@ -31,17 +31,16 @@ struct pk_ctx {
     float4* xs_pre = nullptr;
     float4* xs0 = nullptr;
     float4* xa = nullptr;
-    float4* xb = nullptr;
+    float4* xb = nullptr;     // (x, lambda) written by pass A
     float4* vs = nullptr;
-    float* lam = nullptr;
     float* rho = nullptr;
     int2* rcnt = nullptr;
     uint2* tau = nullptr;
 
     // ---- rows (capacity cap_rows entries)
     long long cap_rows = 0;
-    int* rows = nullptr;
-    float* hitd = nullptr;    // squared distance of each hit-row entry (capped lists)
+    int* rows = nullptr;      // solver rows: sorted index | flag bits
+    uint2* hits = nullptr;    // hit rows: (sorted index, d2 bits), candidate order
 
     // ---- dense cell table (capacity cap_keys entries + 2)
     long long cap_keys = 0;

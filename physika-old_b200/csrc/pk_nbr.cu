@@ -74,8 +74,7 @@ struct BuildArgs {
     Grid g;
     int n, row_cap;
     float T;            // d2 threshold of d < h
-    int* rows;          // hit rows: sorted indices, candidate order
-    float* hitd;        // d2 of each hit, or null (uncapped lists need none)
+    uint2* hits;        // hit rows: (sorted index, d2 bits), candidate order
     int* hcnt;          // hits per particle (sorted order)
     int* count_c;       // hits per particle in caller order (dynamic public list), or null
     const int* perm;
@@ -109,6 +108,32 @@ __device__ __forceinline__ float4 fetch_cand(const float4* __restrict__ xs, cons
     return __ldg(xs + t);
 }
 
+// One pass of the sweep: kPB particles in registers against every candidate
+// chunk.  kChecked guards the row bound; a cell whose 27 ranges hold at most
+// row_cap candidates cannot overflow a row and runs unchecked.
+template <bool kChecked>
+__device__ __forceinline__ void sweep(const BuildArgs& A, const SweepSmem& S, int total, int p0, int m,
+                                      const float (&px)[kPB], const float (&py)[kPB], const float (&pz)[kPB],
+                                      int (&cnt)[kPB], int lane, unsigned lt)
+{
+    uint2* const row0 = A.hits + (long long)p0 * A.row_cap;
+    for (int c0 = 0; c0 < total; c0 += 32) {
+        int t;
+        const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
+#pragma unroll
+        for (int p = 0; p < kPB; ++p) {
+            if (p >= m) break;  // warp-uniform
+            const float d2 = exact_d2(make_float4(px[p], py[p], pz[p], 0.f), cx);
+            const bool hit = d2 < A.T;
+            const unsigned b = __ballot_sync(kFull, hit);
+            const int pos = cnt[p] + __popc(b & lt);
+            if (hit && (!kChecked || pos < A.row_cap))
+                row0[p * A.row_cap + pos] = make_uint2((unsigned)t, __float_as_uint(d2));
+            cnt[p] += __popc(b);
+        }
+    }
+}
+
 // Hit rows, one warp per occupied cell in passes of up to kPB particles.
 // Every lane holds the pass's particles in registers and takes one candidate
 // of each 32-wide chunk of the 27 neighbour ranges: up to kPB independent
@@ -122,7 +147,6 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
     SweepSmem& S = reinterpret_cast<SweepSmem*>(smem_i)[w];
     const int nitems = *A.nitems;
     const int gw = blockIdx.x * kBuildWarps + w, nw = gridDim.x * kBuildWarps;
-    const bool want_d = A.hitd != nullptr;
     for (int item = gw; item < nitems; item += nw) {
         const int2 rng = A.items[item];
         const float4 x0 = A.xs[rng.x];
@@ -165,25 +189,10 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
                 }
                 cnt[p] = 0;
             }
-            int* const row0 = A.rows + (long long)p0 * A.row_cap;
-            float* const d0 = want_d ? A.hitd + (long long)p0 * A.row_cap : nullptr;
-            for (int c0 = 0; c0 < total; c0 += 32) {
-                int t;
-                const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
-#pragma unroll
-                for (int p = 0; p < kPB; ++p) {
-                    if (p >= m) break;  // warp-uniform
-                    const float d2 = exact_d2(make_float4(px[p], py[p], pz[p], 0.f), cx);
-                    const bool hit = d2 < A.T;
-                    const unsigned b = __ballot_sync(kFull, hit);
-                    const int pos = cnt[p] + __popc(b & lt);
-                    if (hit && pos < A.row_cap) {
-                        row0[p * A.row_cap + pos] = t;
-                        if (want_d) d0[p * A.row_cap + pos] = d2;
-                    }
-                    cnt[p] += __popc(b);
-                }
-            }
+            if (total <= A.row_cap)
+                sweep<false>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
+            else
+                sweep<true>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
 #pragma unroll
             for (int p = 0; p < kPB; ++p) {
                 if (lane == p && p < m) {
@@ -199,30 +208,25 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
 
 // ---- tau_i: the cap-th smallest key (d2, sorted index) of each hit row.
 constexpr int kSelWarps = 8;
-constexpr int kSelLevels = 5;  // bins of T/32^5: a few ulps of d2 near T
 
 struct SelSmem {
     int hist[kBins];
-    float sd[32];
-    int st[32];
+    unsigned bmin[kBins], bmax[kBins];  // d2 bits (positive floats order as integers)
+    uint2 slot[32];
 };
 
-// Bin of d2 at one refinement level: kBins equal bins of width 1/scale from
-// lo, clamped; monotone in d2, so bins never reorder keys.
-__device__ __forceinline__ int level_bin(float d2, float lo, float scale)
-{
-    return min(max((int)((d2 - lo) * scale), 0), kBins - 1);
-}
-
-// One warp per particle whose row holds more than cap hits.  Histogram
-// refinement over the row's stored d2: a 32-bin histogram of the hits in play
-// locates the bin holding the rank, whose hits are the next level's play set;
-// once the bin holds at most 32 hits they are ranked exactly by (d2, index).
-// Bins are monotone in d2, so each play set is an interval of keys.  Hits at
-// d2 values no split separates are ranked against the whole play set.
+// One warp per particle whose row holds more than cap hits.  The hits in
+// play always form an interval [plo, phi] of d2 values (initially all of
+// them).  While more than 32 are in play, a 32-bin histogram over the
+// interval, with each bin's smallest and largest d2, locates the bin holding
+// the wanted rank; that bin's extreme values are the next interval.  Bins are
+// monotone in d2, so an interval's hits are exactly the bin's hits, and plo
+// falls in bin 0 while phi falls in the last bin: every level shrinks the set.
+// At most 32 hits left are ranked exactly by (d2, index); a set of more than
+// 32 hits at one d2 value is ranked by index directly.
 __global__ void __launch_bounds__(kSelWarps * 32)
-    k_select(const int* __restrict__ rows, const float* __restrict__ hitd, const int* __restrict__ hcnt,
-             int n, int cap, int row_cap, float bin_scale, uint2* __restrict__ tau)
+    k_select(const uint2* __restrict__ hits, const int* __restrict__ hcnt, int n, int cap, int row_cap,
+             float T, uint2* __restrict__ tau)
 {
     __shared__ SelSmem sm[kSelWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -230,103 +234,89 @@ __global__ void __launch_bounds__(kSelWarps * 32)
     SelSmem& S = sm[w];
     const int gw = blockIdx.x * kSelWarps + w, nw = gridDim.x * kSelWarps;
     for (int s = gw; s < n; s += nw) {
-        const int c = hcnt[s];
+        const int c = __ldg(hcnt + s);
         uint2 res = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
         if (c > cap) {
-            const int* row = rows + (long long)s * row_cap;
-            const float* rd = hitd + (long long)s * row_cap;
-            float lo[kSelLevels], sc[kSelLevels];
-            int bsel[kSelLevels];
-            int rr = cap - 1;
-            bool done = false;
-            lo[0] = 0.f;
-            sc[0] = bin_scale;
-#pragma unroll
-            for (int L = 0; L < kSelLevels; ++L) {
-                if (!done) {
-                    S.hist[lane] = 0;
-                    __syncwarp();
-                    for (int e0 = 0; e0 < c; e0 += 32) {
-                        const int e = e0 + lane;
-                        if (e < c) {
-                            const float d2 = __ldg(rd + e);
-                            bool in = true;
-#pragma unroll
-                            for (int q = 0; q < L; ++q) in = in && level_bin(d2, lo[q], sc[q]) == bsel[q];
-                            if (in) atomicAdd(&S.hist[level_bin(d2, lo[L], sc[L])], 1);
-                        }
+            const uint2* row = hits + (long long)s * row_cap;
+            unsigned plo = 0u, phi = __float_as_uint(T);  // [0, T]: every hit
+            float lo = 0.f, scale = (float)kBins / T;
+            int rr = cap - 1, np = c;
+            while (np > 32 && plo != phi) {
+                S.hist[lane] = 0;
+                S.bmin[lane] = 0xffffffffu;
+                S.bmax[lane] = 0u;
+                __syncwarp();
+                for (int e = lane; e < c; e += 32) {
+                    const unsigned db = __ldg(row + e).y;
+                    if (db >= plo && db <= phi) {
+                        const int b = min(max((int)((__uint_as_float(db) - lo) * scale), 0), kBins - 1);
+                        atomicAdd(&S.hist[b], 1);
+                        atomicMin(&S.bmin[b], db);
+                        atomicMax(&S.bmax[b], db);
                     }
-                    __syncwarp();
-                    const int h = S.hist[lane];
-                    int incl = h;
+                }
+                __syncwarp();
+                const int h = S.hist[lane];
+                int incl = h;
 #pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(kFull, incl, o);
-                        if (lane >= o) incl += y;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int B = __ffs(__ballot_sync(kFull, incl > rr)) - 1;
+                np = __shfl_sync(kFull, h, B);
+                rr -= __shfl_sync(kFull, incl - h, B);
+                plo = S.bmin[B];
+                phi = S.bmax[B];
+                __syncwarp();
+                lo = __uint_as_float(plo);
+                const float width = __uint_as_float(phi) - lo;
+                scale = width > 0.f ? (float)kBins / width : 0.f;
+            }
+            uint2 mine = make_uint2(0u, 0x7fffffffu);
+            if (np <= 32) {
+                // collect the play set, then rank each member against the others
+                int k = 0;
+                for (int e0 = 0; e0 < c; e0 += 32) {
+                    const int e = e0 + lane;
+                    uint2 h = make_uint2(0u, 0u);
+                    bool in = false;
+                    if (e < c) {
+                        h = __ldg(row + e);
+                        in = h.y >= plo && h.y <= phi;
                     }
-                    const int B = __ffs(__ballot_sync(kFull, incl > rr)) - 1;
-                    const int nB = __shfl_sync(kFull, h, B);
-                    rr -= __shfl_sync(kFull, incl - h, B);
-                    bsel[L] = B;
-                    if (L + 1 < kSelLevels) {
-                        lo[L + 1] = lo[L] + (float)B / sc[L];
-                        sc[L + 1] = sc[L] * (float)kBins;
+                    const unsigned bal = __ballot_sync(kFull, in);
+                    if (in) S.slot[k + __popc(bal & lt)] = h;
+                    k += __popc(bal);
+                }
+                __syncwarp();
+                if (lane < k) {
+                    const uint2 me = S.slot[lane];
+                    int rank = 0;
+                    for (int u = 0; u < k; ++u) {
+                        const uint2 o = S.slot[u];
+                        rank += (o.y < me.y || (o.y == me.y && o.x < me.x)) ? 1 : 0;
                     }
-                    if (nB <= 32 || L + 1 == kSelLevels) {
-                        // the play set of the next level, ranked exactly
-                        const bool small = nB <= 32;
-                        int k = 0;
-                        uint2 mine = make_uint2(0x7f800000u, 0x7fffffffu);
-                        for (int e0 = 0; e0 < c; e0 += 32) {
-                            const int e = e0 + lane;
-                            float d2 = 0.f;
-                            int t = 0;
-                            bool in = false;
-                            if (e < c) {
-                                d2 = __ldg(rd + e);
-                                t = __ldg(row + e);
-                                in = true;
-#pragma unroll
-                                for (int q = 0; q <= L; ++q) in = in && level_bin(d2, lo[q], sc[q]) == bsel[q];
-                            }
-                            if (small) {
-                                const unsigned bal = __ballot_sync(kFull, in);
-                                if (in) {
-                                    const int q = k + __popc(bal & lt);
-                                    S.sd[q] = d2;
-                                    S.st[q] = t;
-                                }
-                                k += __popc(bal);
-                            } else if (in) {
-                                // rank this hit against the whole play set
-                                int rank = 0;
-                                for (int u = 0; u < c; ++u) {
-                                    const float du = __ldg(rd + u);
-                                    bool inu = true;
-#pragma unroll
-                                    for (int q = 0; q <= L; ++q) inu = inu && level_bin(du, lo[q], sc[q]) == bsel[q];
-                                    if (inu) rank += key_lt(du, __ldg(row + u), d2, t);
-                                }
-                                if (rank == rr) mine = make_uint2(__float_as_uint(d2), (unsigned)t);
-                            }
-                        }
-                        __syncwarp();
-                        if (small && lane < k) {
-                            const float dm = S.sd[lane];
-                            const int tm = S.st[lane];
-                            int rank = 0;
-                            for (int u = 0; u < k; ++u) rank += key_lt(S.sd[u], S.st[u], dm, tm);
-                            if (rank == rr) mine = make_uint2(__float_as_uint(dm), (unsigned)tm);
-                        }
-                        const unsigned f = __ballot_sync(kFull, mine.y != 0x7fffffffu);
-                        const int src = f ? __ffs(f) - 1 : 0;
-                        res.x = __shfl_sync(kFull, mine.x, src);
-                        res.y = __shfl_sync(kFull, mine.y, src);
-                        done = true;
+                    if (rank == rr) mine = make_uint2(me.y, me.x);
+                }
+            } else {
+                // more than 32 hits at one d2 value: the rr-th smallest index
+                for (int e = lane; e < c; e += 32) {
+                    const uint2 h = __ldg(row + e);
+                    if (h.y != plo) continue;
+                    int rank = 0;
+                    for (int u = 0; u < c; ++u) {
+                        const uint2 o = __ldg(row + u);
+                        rank += (o.y == plo && o.x < h.x) ? 1 : 0;
                     }
-                    __syncwarp();
+                    if (rank == rr) mine = make_uint2(h.y, h.x);
                 }
             }
+            const unsigned f = __ballot_sync(kFull, mine.y != 0x7fffffffu);
+            const int src = f ? __ffs(f) - 1 : 0;
+            res.x = __shfl_sync(kFull, mine.x, src);
+            res.y = __shfl_sync(kFull, mine.y, src);
+            __syncwarp();
         }
         if (lane == 0) tau[s] = res;
     }
@@ -337,7 +327,7 @@ constexpr int kEmitG = 8;
 constexpr int kStash = 128;  // b-only entries kept per group before appending
 
 __global__ void __launch_bounds__(256)
-    k_emit(const int* __restrict__ hcnt, const float* __restrict__ hitd, const uint2* __restrict__ tau,
+    k_emit(const int* __restrict__ hcnt, const uint2* __restrict__ hits, const uint2* __restrict__ tau,
            const int* __restrict__ perm, int n, int cap, int row_cap, int* __restrict__ rows,
            int2* __restrict__ rcnt, int* __restrict__ pub_index, int* __restrict__ pub_elements,
            long long pub_capacity, const int* __restrict__ offs, int* __restrict__ err)
@@ -361,7 +351,7 @@ __global__ void __launch_bounds__(256)
         if (pub) pbase = capped ? (long long)ps * cap : (long long)offs[ps];
     }
     int* row = rows + (long long)(valid ? s : 0) * row_cap;
-    const float* rd = capped ? hitd + (long long)(valid ? s : 0) * row_cap : nullptr;
+    const uint2* hrow = hits + (long long)(valid ? s : 0) * row_cap;
     // every lane of the warp iterates to the longest row of the warp's groups
     int cmax = cnt;
 #pragma unroll
@@ -373,9 +363,10 @@ __global__ void __launch_bounds__(256)
         bool fa = false, fb = false;
         int t = 0;
         if (valid && e < cnt) {
-            t = row[e];
+            const uint2 h = __ldg(hrow + e);
+            t = (int)h.x;
             if (capped) {
-                const float d2 = rd[e];
+                const float d2 = __uint_as_float(h.y);
                 fa = key_le(d2, t, ti);
                 fb = key_le(d2, s, __ldg(tau + t));
             } else {
@@ -384,7 +375,6 @@ __global__ void __launch_bounds__(256)
         }
         const unsigned ba = __ballot_sync(kFull, fa) & gmask;
         const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
-        // entries only move towards the front, never onto unread ones
         if (fa) {
             const int q = nA + __popc(ba & lt_g);
             row[q] = t | kRowFlagA | (fb ? kRowFlagB : 0);
@@ -451,8 +441,7 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     A.n = n;
     A.row_cap = row_cap;
     A.T = radius_threshold(h);
-    A.rows = c->rows;
-    A.hitd = capped ? c->hitd : nullptr;
+    A.hits = c->hits;
     A.hcnt = c->hcnt;
     A.count_c = dyn_pub ? c->count_c : nullptr;
     A.perm = c->perm;
@@ -463,8 +452,7 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     ++launches;
     if (capped) {
         const int sb = std::min((n + kSelWarps - 1) / kSelWarps, sms * 8);
-        k_select<<<sb, kSelWarps * 32, 0, st>>>(c->rows, c->hitd, c->hcnt, n, cap, row_cap,
-                                                (float)kBins / A.T, c->tau);
+        k_select<<<sb, kSelWarps * 32, 0, st>>>(c->hits, c->hcnt, n, cap, row_cap, A.T, c->tau);
         ++launches;
     }
     if (dyn_pub) {
@@ -474,7 +462,7 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     prof_end(c, PK_PROF_SELECT, st);
     prof_begin(c, PK_PROF_EMIT, st);
     const unsigned ne = (unsigned)(((long long)n * kEmitG + 255) / 256);
-    k_emit<<<ne, 256, 0, st>>>(c->hcnt, c->hitd, c->tau, c->perm, n, cap, row_cap, c->rows, c->rcnt,
+    k_emit<<<ne, 256, 0, st>>>(c->hcnt, c->hits, c->tau, c->perm, n, cap, row_cap, c->rows, c->rcnt,
                                pub_index, pub_elements, pub_capacity, c->offs, c->d_err);
     prof_end(c, PK_PROF_EMIT, st);
     return launches + 1;

@@ -11,7 +11,8 @@
 //           (+dp_ij to i, -dp_ij to j, DensityPBD.cu:134-179) accumulates,
 //           since dp_ji = -dp_ij bit for bit.
 // G lanes share one particle: each takes every G-th row entry, partial sums
-// are combined with xor shuffles.  x is ping-ponged (Jacobi).
+// are combined with xor shuffles.  Jacobi: pass A reads x, writes (x, lambda)
+// to xl; pass B reads xl only and writes x'.
 #include "pk_kernels.cuh"
 
 namespace pk {
@@ -26,36 +27,60 @@ __device__ __forceinline__ float group_sum(float v)
     return v;
 }
 
+// Per-pair constants of the two passes (Spiky kernel, Kernel.h SpikyKernel).
+struct PassK {
+    float inv_h, cwm, cg, c10g;
+};
+__host__ __device__ inline PassK pass_k(const Spiky& k, float mass)
+{
+    return PassK{k.inv_h, mass * k.cw, k.cg, 10.0f * k.cg};
+}
+constexpr float kEps2 = kEpsilon * kEpsilon;  // r > EPSILON  <=>  r^2 > EPSILON^2
+
+// Pair geometry shared by both passes: r from one reciprocal square root
+// (r = d2 / sqrt(d2); d2 = 0 gives r = 0), 1/r, and d = 1 - r/h clamped at 0,
+// so w = cw d^3 and |grad| = cg d^2 vanish beyond h as in SpikyKernel.
+__device__ __forceinline__ void pair_geom(float dx, float dy, float dz, float inv_h, float& d2, float& ir,
+                                          float& dd)
+{
+    d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    ir = rsqrtf(fmaxf(d2, 1e-30f));
+    dd = fmaxf(fmaf(-(d2 * ir), inv_h, 1.0f), 0.0f);
+}
+
+// Pass A: rho_i and lambda_i over N(i).  Writes xl[s] = (x_i, lambda_i) so
+// pass B gathers a neighbour's position and lambda in one 16-byte load.
+// sum |grad_j|^2 is taken as sum g_j^2 (|x_ij / r| = 1).
 template <int G>
 __global__ void __launch_bounds__(256)
     k_pass_density(const float4* __restrict__ xs, const int* __restrict__ rows,
-                   const int2* __restrict__ rcnt, int row_cap, int n, Spiky k, float mass,
-                   float* __restrict__ lam, float* __restrict__ rho_out)
+                   const int2* __restrict__ rcnt, int row_cap, int n, PassK k,
+                   float4* __restrict__ xl, float* __restrict__ rho_out)
 {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = gid / G, sub = gid % G;
     const bool valid = s < n;
     float rho = 0.f, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-        const float4 xi = xs[s];
+        xi = xs[s];
         const int na = rcnt[s].x;
         const int* row = rows + (long long)s * row_cap;
+#pragma unroll 2
         for (int e = sub; e < na; e += G) {
             const int j = __ldg(row + e) & kRowIndexMask;
             const float4 xj = __ldg(xs + j);
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const float r = sqrtf(dx * dx + dy * dy + dz * dz);
-            float w, g;
-            spiky_wg(k, r, w, g);
-            rho += mass * w;
-            if (r > kEpsilon) {
-                const float ir = 1.0f / r;
-                const float g0 = g * dx * ir, g1 = g * dy * ir, g2 = g * dz * ir;
-                gx += g0;
-                gy += g1;
-                gz += g2;
-                sg += g0 * g0 + g1 * g1 + g2 * g2;
-            }
+            float d2, ir, dd;
+            pair_geom(dx, dy, dz, k.inv_h, d2, ir, dd);
+            const float dd2 = dd * dd;
+            rho = fmaf(k.cwm, dd2 * dd, rho);
+            const float g = d2 > kEps2 ? k.cg * dd2 : 0.0f;
+            const float gi = g * ir;
+            gx = fmaf(gi, dx, gx);
+            gy = fmaf(gi, dy, gy);
+            gz = fmaf(gi, dz, gz);
+            sg = fmaf(g, g, sg);
         }
     }
     rho = group_sum<G>(rho);
@@ -66,16 +91,18 @@ __global__ void __launch_bounds__(256)
     if (valid && sub == 0) {
         float l = sg + (gx * gx + gy * gy + gz * gz);
         l = -(rho - 1000.0f) / (l + 0.1f);  // rest density hard-coded (DensityPBD.cu:87)
-        lam[s] = l > 0.0f ? 0.0f : l;
+        xl[s] = make_float4(xi.x, xi.y, xi.z, l > 0.0f ? 0.0f : l);
         if (rho_out != nullptr) rho_out[s] = rho;
     }
 }
 
+// Pass B: x_i' = x_i + sum over U(i) of m_ij * 10 (x_i - x_j)(lambda_i +
+// lambda_j) grad(r) / r (DensityPBD.cu:158), m_ij = popcount of the two flag
+// bits.
 template <int G>
 __global__ void __launch_bounds__(256)
-    k_pass_disp(const float4* __restrict__ xs, const float* __restrict__ lam,
-                const int* __restrict__ rows, const int2* __restrict__ rcnt, int row_cap, int n,
-                Spiky k, float4* __restrict__ xs_out)
+    k_pass_disp(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
+                int row_cap, int n, PassK k, float4* __restrict__ xs_out)
 {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = gid / G, sub = gid % G;
@@ -83,27 +110,22 @@ __global__ void __launch_bounds__(256)
     float ax = 0.f, ay = 0.f, az = 0.f;
     float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-        xi = xs[s];
-        const float li = lam[s];
+        xi = xl[s];
         const int nu = rcnt[s].y;
         const int* row = rows + (long long)s * row_cap;
+#pragma unroll 2
         for (int e = sub; e < nu; e += G) {
             const int v = __ldg(row + e);
             const int j = v & kRowIndexMask;
-            const float mult = (float)(((unsigned)v >> 31) + (((unsigned)v >> 30) & 1u));
-            const float4 xj = __ldg(xs + j);
+            const float mult = (float)__popc((unsigned)v >> 30);
+            const float4 xj = __ldg(xl + j);
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const float r = sqrtf(dx * dx + dy * dy + dz * dz);
-            if (r > kEpsilon) {
-                float w, g;
-                spiky_wg(k, r, w, g);
-                const float sl = li + __ldg(lam + j);
-                const float ir = 1.0f / r;
-                // 10*(x_i - x_j)*(lambda_i + lambda_j)*grad*(1/r) (DensityPBD.cu:158)
-                ax += mult * (10.0f * dx * sl * g * ir);
-                ay += mult * (10.0f * dy * sl * g * ir);
-                az += mult * (10.0f * dz * sl * g * ir);
-            }
+            float d2, ir, dd;
+            pair_geom(dx, dy, dz, k.inv_h, d2, ir, dd);
+            const float c = d2 > kEps2 ? mult * (xi.w + xj.w) * (k.c10g * (dd * dd)) * ir : 0.0f;
+            ax = fmaf(c, dx, ax);
+            ay = fmaf(c, dy, ay);
+            az = fmaf(c, dz, az);
         }
     }
     ax = group_sum<G>(ax);
@@ -154,17 +176,19 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     const unsigned nbg = (unsigned)(((long long)n * kGroup + 255) / 256);
     int launches = 0;
     const float4* cur = c->xs0;
+    const PassK pk = pass_k(k, mass);
+    // pass B reads only xl, so it may overwrite the positions pass A read
+    // (except xs0, which the velocity update needs)
     for (int it = 0; it < iterations; ++it) {
-        float4* nxt = (it & 1) ? c->xb : c->xa;
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
-        k_pass_density<kGroup><<<nbg, 256, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, k, mass,
-                                                    c->lam, last ? c->rho : nullptr);
+        k_pass_density<kGroup><<<nbg, 256, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                                    last ? c->rho : nullptr);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
-        k_pass_disp<kGroup><<<nbg, 256, 0, st>>>(cur, c->lam, c->rows, c->rcnt, c->row_cap, n, k, nxt);
+        k_pass_disp<kGroup><<<nbg, 256, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
         prof_end(c, PK_PROF_DISP, st);
-        cur = nxt;
+        cur = c->xa;
         launches += 2;
     }
     prof_begin(c, PK_PROF_FINISH, st);
