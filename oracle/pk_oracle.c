@@ -479,6 +479,20 @@ void pko_sdf_constrain(int n, float* x, float* v, const pko_sdf* s, const float*
 #undef SFX
 #undef RSQRT
 
+/* The float kernel functions the solver uses, for checking against the
+ * reference's compiled SpikyKernel / SmoothKernel / CorrectedKernel. */
+void pko_kernels_f(int n, const float* r, float h, float* out5)
+{
+    int i;
+    for (i = 0; i < n; i++) {
+        out5[5 * i + 0] = spiky_w_f(r[i], h);
+        out5[5 * i + 1] = spiky_g_f(r[i], h);
+        out5[5 * i + 2] = smooth_w_f(r[i], h);
+        out5[5 * i + 3] = corr_w_f(r[i], h);
+        out5[5 * i + 4] = corr_wrr_f(r[i], h);
+    }
+}
+
 #define real double
 #define SFX(name) name##_d
 #define RSQRT sqrt

@@ -10,6 +10,16 @@
  * Every function restates one reference kernel or host routine and cites the
  * reference file:line it follows (paths relative to the PhysIKA source tree).
  *
+ * Pinning: the reference's hot-path translation units do not compile outside
+ * MSVC (oracle/Makefile says where), so the reference is not run end to end.
+ * Its own compiled arithmetic is: oracle/_ref/ref_math_probe builds the
+ * reference's Vector3f::norm/normalize and Kernel.h from the reference
+ * sources, and tests/golden/ref_math.npz holds its outputs on a B200.  The
+ * distance (norm variant 1) and the Spiky / Smooth / Corrected kernels here
+ * reproduce those bit for bit (tests/test_golden_ref_cpu.py); the control
+ * flow around them (grid, 27-cell walk, cap selection, Jacobi passes) is
+ * restated from the source and is not pinned by a reference run.
+ *
  * Precision: the neighbour query, grid and SDF are float only (the reference
  * computes them in float).  The solver functions exist in two builds of the
  * same source: suffix _f (float, the reference's precision) and _d (double,
@@ -37,11 +47,16 @@ typedef struct {
 
 void  pko_grid_setup(pko_grid* g, float h, const float lo[3], const float hi[3]);
 /* Which float expression computes |a-b|.  0: ((x*x+y*y)+z*z), 1:
- * fma(z,z,fma(x,x,y*y)), 2: fma(z,z,fma(y,y,x*x)).  Must equal the variant the
- * CUDA library was built with for neighbour sets to be bit-exact. */
+ * fma(z,z,fma(x,x,y*y)), 2: fma(z,z,fma(y,y,x*x)).  1 (the default) is what
+ * the reference's Vector3f::norm compiles to under nvcc (pinned by
+ * tests/golden/ref_math.npz); it must equal the variant the CUDA library was
+ * built with for neighbour sets to be bit-exact. */
 void  pko_set_norm_variant(int v);
 int   pko_get_norm_variant(void);
 float pko_dist3(const float* a, const float* b);
+/* SpikyKernel Weight/Gradient, SmoothKernel::Weight, CorrectedKernel
+ * Weight/WeightRR (Kernel.h:29-142) at radii r[n], float: out5[5*i + k]. */
+void  pko_kernels_f(int n, const float* r, float h, float* out5);
 
 /* NeighborQuery::compute (NeighborQuery.cu:152-199) with GridHash::construct
  * (GridHash.cu:297-323).  Fixed mode (cap > 0) follows K_ComputeNeighborFixed

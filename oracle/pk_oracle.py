@@ -32,6 +32,7 @@ def lib():
         L.pko_max_threads.restype = c_int
         L.pko_dist3.argtypes = [_f32p, _f32p]
         L.pko_dist3.restype = c_float
+        L.pko_kernels_f.argtypes = [c_int, _f32p, c_float, _f32p]
         L.pko_neighbor_query.argtypes = [c_int, _f32p, c_float, _f32p, _f32p, c_int,
                                          ctypes.c_void_p, ctypes.c_void_p, c_ll,
                                          ctypes.POINTER(c_ll)]
@@ -77,6 +78,22 @@ def max_threads():
 
 def dist3(a, b):
     return lib().pko_dist3(np.ascontiguousarray(a, np.float32), np.ascontiguousarray(b, np.float32))
+
+
+def dist3_many(pairs):
+    """|a - b| for each row (a, b) of an (n, 6) float32 array."""
+    p = np.ascontiguousarray(pairs, np.float32)
+    L = lib()
+    return np.array([L.pko_dist3(np.ascontiguousarray(q[:3]), np.ascontiguousarray(q[3:])) for q in p],
+                    np.float32)
+
+
+def kernels(r, h):
+    """(n, 5): SpikyKernel W, G; SmoothKernel W; CorrectedKernel W, WRR (float)."""
+    r = np.ascontiguousarray(r, np.float32)
+    out = np.zeros((r.shape[0], 5), np.float32)
+    lib().pko_kernels_f(r.shape[0], r, float(h), out)
+    return out
 
 
 def _v3(a):

@@ -36,11 +36,20 @@ def build_pkhot(force=False, verbose=True):
     return out
 
 
-def build_oracle(verbose=True):
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True,
-                   stdout=None if verbose else subprocess.DEVNULL)
+REFERENCE = os.environ.get("PK_REFERENCE_SRC", "/root/reference")
+
+
+def build_oracle(verbose=True, with_ref=False):
+    """The CPU restatement; with_ref also builds the golden-vector driver
+    oracle/_ref/ref_math_probe from the reference sources when they are present
+    (they are not on a GPU machine, which uses the prebuilt driver)."""
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True, stdout=out)
+    if with_ref and os.path.isdir(os.path.join(REFERENCE, "Source")):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + REFERENCE],
+                       check=True, stdout=out)
 
 
 if __name__ == "__main__":
     build_pkhot(force="--force" in sys.argv)
-    build_oracle()
+    build_oracle(with_ref=True)

@@ -208,22 +208,135 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
 
 // ---- tau_i: the cap-th smallest key (d2, sorted index) of each hit row.
 constexpr int kSelWarps = 8;
+constexpr int kSelRegChunks = 4;  // rows of up to 128 hits are held in registers
 
 struct SelSmem {
     int hist[kBins];
-    unsigned bmin[kBins], bmax[kBins];  // d2 bits (positive floats order as integers)
     uint2 slot[32];
 };
 
-// One warp per particle whose row holds more than cap hits.  The hits in
-// play always form an interval [plo, phi] of d2 values (initially all of
-// them).  While more than 32 are in play, a 32-bin histogram over the
-// interval, with each bin's smallest and largest d2, locates the bin holding
-// the wanted rank; that bin's extreme values are the next interval.  Bins are
-// monotone in d2, so an interval's hits are exactly the bin's hits, and plo
-// falls in bin 0 while phi falls in the last bin: every level shrinks the set.
-// At most 32 hits left are ranked exactly by (d2, index); a set of more than
-// 32 hits at one d2 value is ranked by index directly.
+__device__ __forceinline__ int sel_bin(unsigned db, float lo, float scale)
+{
+    return min(max((int)((__uint_as_float(db) - lo) * scale), 0), kBins - 1);
+}
+
+// Rank rr (0-based) among the c keys of a row, one warp.  The hits in play
+// always form an interval [plo, phi] of d2 values (initially all of them).
+// While more than 32 are in play, a 32-bin histogram over the interval
+// locates the bin holding the rank, and that bin's smallest and largest d2
+// become the next interval.  Bins are monotone in d2, so an interval's hits
+// are exactly its bin's hits, and plo falls in bin 0 while phi falls in the
+// last bin: every level shrinks the set.  At most 32 hits left are ranked
+// exactly by (d2, index); more than 32 hits at one d2 value are ranked by
+// index.  Src supplies the row: chunk k of 32 entries (lanes past c hold
+// d2 bits 0xffffffff, outside every interval).
+template <class Src>
+__device__ __forceinline__ uint2 select_rank(const Src& src, int nch, const uint2* __restrict__ row, int c, int rr, float T,
+                             SelSmem& S, int lane, unsigned lt)
+{
+    unsigned plo = 0u, phi = __float_as_uint(T);  // [0, T]: every hit
+    float lo = 0.f, scale = (float)kBins / T;
+    int np = c;
+    while (np > 32 && plo != phi) {
+        S.hist[lane] = 0;
+        __syncwarp();
+        for (int k = 0; k < nch; ++k) {
+            const uint2 v = src(k);
+            if (v.y >= plo && v.y <= phi) atomicAdd(&S.hist[sel_bin(v.y, lo, scale)], 1);
+        }
+        __syncwarp();
+        const int hb = S.hist[lane];
+        int incl = hb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int B = __ffs(__ballot_sync(kFull, incl > rr)) - 1;
+        np = __shfl_sync(kFull, hb, B);
+        rr -= __shfl_sync(kFull, incl - hb, B);
+        // the chosen bin's extreme values
+        unsigned mn = 0xffffffffu, mx = 0u;
+        for (int k = 0; k < nch; ++k) {
+            const uint2 v = src(k);
+            if (v.y >= plo && v.y <= phi && sel_bin(v.y, lo, scale) == B) {
+                mn = min(mn, v.y);
+                mx = max(mx, v.y);
+            }
+        }
+        plo = __reduce_min_sync(kFull, mn);
+        phi = __reduce_max_sync(kFull, mx);
+        lo = __uint_as_float(plo);
+        const float width = __uint_as_float(phi) - lo;
+        scale = width > 0.f ? (float)kBins / width : 0.f;
+        __syncwarp();
+    }
+    uint2 mine = make_uint2(0u, 0x7fffffffu);
+    if (np <= 32) {
+        int k = 0;
+        for (int q = 0; q < nch; ++q) {
+            const uint2 v = src(q);
+            const bool in = v.y >= plo && v.y <= phi;
+            const unsigned bal = __ballot_sync(kFull, in);
+            if (in) S.slot[k + __popc(bal & lt)] = v;
+            k += __popc(bal);
+        }
+        __syncwarp();
+        if (lane < k) {
+            const uint2 me = S.slot[lane];
+            int rank = 0;
+            for (int u = 0; u < k; ++u) {
+                const uint2 o = S.slot[u];
+                rank += (o.y < me.y || (o.y == me.y && o.x < me.x)) ? 1 : 0;
+            }
+            if (rank == rr) mine = make_uint2(me.y, me.x);
+        }
+    } else {
+        // more than 32 hits at one d2 value: the rr-th smallest index
+        for (int e = lane; e < c; e += 32) {
+            const uint2 v = __ldg(row + e);
+            if (v.y != plo) continue;
+            int rank = 0;
+            for (int u = 0; u < c; ++u) {
+                const uint2 o = __ldg(row + u);
+                rank += (o.y == plo && o.x < v.x) ? 1 : 0;
+            }
+            if (rank == rr) mine = make_uint2(v.y, v.x);
+        }
+    }
+    const unsigned f = __ballot_sync(kFull, mine.y != 0x7fffffffu);
+    const int sl = f ? __ffs(f) - 1 : 0;
+    __syncwarp();
+    return make_uint2(__shfl_sync(kFull, mine.x, sl), __shfl_sync(kFull, mine.y, sl));
+}
+
+// Row chunks from registers (rows of at most 32 * kSelRegChunks hits).
+struct RegSrc {
+    uint2 h[kSelRegChunks];
+    __device__ __forceinline__ uint2 operator()(int k) const
+    {
+        uint2 v = h[0];
+#pragma unroll
+        for (int q = 1; q < kSelRegChunks; ++q)
+            if (k == q) v = h[q];
+        return v;
+    }
+};
+// Row chunks from memory (longer rows).
+struct MemSrc {
+    const uint2* row;
+    int c, lane;
+    __device__ __forceinline__ uint2 operator()(int k) const
+    {
+        const int e = k * 32 + lane;
+        return e < c ? __ldg(row + e) : make_uint2(0u, 0xffffffffu);
+    }
+};
+
+// A warp takes 32 consecutive particles: lane l reads the count of particle
+// base + l, the particles with more than cap hits are selected one after the
+// other (their rows loaded into registers when they hold at most 128 hits),
+// and lane l writes tau of particle base + l.
 __global__ void __launch_bounds__(kSelWarps * 32)
     k_select(const uint2* __restrict__ hits, const int* __restrict__ hcnt, int n, int cap, int row_cap,
              float T, uint2* __restrict__ tau)
@@ -232,93 +345,32 @@ __global__ void __launch_bounds__(kSelWarps * 32)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     SelSmem& S = sm[w];
-    const int gw = blockIdx.x * kSelWarps + w, nw = gridDim.x * kSelWarps;
-    for (int s = gw; s < n; s += nw) {
-        const int c = __ldg(hcnt + s);
-        uint2 res = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
-        if (c > cap) {
-            const uint2* row = hits + (long long)s * row_cap;
-            unsigned plo = 0u, phi = __float_as_uint(T);  // [0, T]: every hit
-            float lo = 0.f, scale = (float)kBins / T;
-            int rr = cap - 1, np = c;
-            while (np > 32 && plo != phi) {
-                S.hist[lane] = 0;
-                S.bmin[lane] = 0xffffffffu;
-                S.bmax[lane] = 0u;
-                __syncwarp();
-                for (int e = lane; e < c; e += 32) {
-                    const unsigned db = __ldg(row + e).y;
-                    if (db >= plo && db <= phi) {
-                        const int b = min(max((int)((__uint_as_float(db) - lo) * scale), 0), kBins - 1);
-                        atomicAdd(&S.hist[b], 1);
-                        atomicMin(&S.bmin[b], db);
-                        atomicMax(&S.bmax[b], db);
-                    }
-                }
-                __syncwarp();
-                const int h = S.hist[lane];
-                int incl = h;
+    const long long gw = (long long)blockIdx.x * kSelWarps + w, nw = (long long)gridDim.x * kSelWarps;
+    for (long long base = gw * 32; base < n; base += nw * 32) {
+        const long long s_l = base + lane;
+        const int c_l = s_l < n ? __ldg(hcnt + s_l) : 0;
+        uint2 tau_l = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
+        unsigned need = __ballot_sync(kFull, c_l > cap);
+        while (need) {
+            const int q = __ffs(need) - 1;
+            need &= need - 1;
+            const int c = __shfl_sync(kFull, c_l, q);
+            const uint2* row = hits + (base + q) * row_cap;
+            uint2 r;
+            if (c <= 32 * kSelRegChunks) {
+                RegSrc src;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(kFull, incl, o);
-                    if (lane >= o) incl += y;
+                for (int k = 0; k < kSelRegChunks; ++k) {
+                    const int e = k * 32 + lane;
+                    src.h[k] = e < c ? __ldg(row + e) : make_uint2(0u, 0xffffffffu);
                 }
-                const int B = __ffs(__ballot_sync(kFull, incl > rr)) - 1;
-                np = __shfl_sync(kFull, h, B);
-                rr -= __shfl_sync(kFull, incl - h, B);
-                plo = S.bmin[B];
-                phi = S.bmax[B];
-                __syncwarp();
-                lo = __uint_as_float(plo);
-                const float width = __uint_as_float(phi) - lo;
-                scale = width > 0.f ? (float)kBins / width : 0.f;
-            }
-            uint2 mine = make_uint2(0u, 0x7fffffffu);
-            if (np <= 32) {
-                // collect the play set, then rank each member against the others
-                int k = 0;
-                for (int e0 = 0; e0 < c; e0 += 32) {
-                    const int e = e0 + lane;
-                    uint2 h = make_uint2(0u, 0u);
-                    bool in = false;
-                    if (e < c) {
-                        h = __ldg(row + e);
-                        in = h.y >= plo && h.y <= phi;
-                    }
-                    const unsigned bal = __ballot_sync(kFull, in);
-                    if (in) S.slot[k + __popc(bal & lt)] = h;
-                    k += __popc(bal);
-                }
-                __syncwarp();
-                if (lane < k) {
-                    const uint2 me = S.slot[lane];
-                    int rank = 0;
-                    for (int u = 0; u < k; ++u) {
-                        const uint2 o = S.slot[u];
-                        rank += (o.y < me.y || (o.y == me.y && o.x < me.x)) ? 1 : 0;
-                    }
-                    if (rank == rr) mine = make_uint2(me.y, me.x);
-                }
+                r = select_rank(src, (c + 31) / 32, row, c, cap - 1, T, S, lane, lt);
             } else {
-                // more than 32 hits at one d2 value: the rr-th smallest index
-                for (int e = lane; e < c; e += 32) {
-                    const uint2 h = __ldg(row + e);
-                    if (h.y != plo) continue;
-                    int rank = 0;
-                    for (int u = 0; u < c; ++u) {
-                        const uint2 o = __ldg(row + u);
-                        rank += (o.y == plo && o.x < h.x) ? 1 : 0;
-                    }
-                    if (rank == rr) mine = make_uint2(h.y, h.x);
-                }
+                r = select_rank(MemSrc{row, c, lane}, (c + 31) / 32, row, c, cap - 1, T, S, lane, lt);
             }
-            const unsigned f = __ballot_sync(kFull, mine.y != 0x7fffffffu);
-            const int src = f ? __ffs(f) - 1 : 0;
-            res.x = __shfl_sync(kFull, mine.x, src);
-            res.y = __shfl_sync(kFull, mine.y, src);
-            __syncwarp();
+            if (lane == q) tau_l = r;
         }
-        if (lane == 0) tau[s] = res;
+        if (s_l < n) tau[s_l] = tau_l;
     }
 }
 
@@ -451,7 +503,7 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     k_build<<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
     ++launches;
     if (capped) {
-        const int sb = std::min((n + kSelWarps - 1) / kSelWarps, sms * 8);
+        const int sb = (int)std::min<long long>(((long long)n + 32 * kSelWarps - 1) / (32 * kSelWarps), (long long)sms * 8);
         k_select<<<sb, kSelWarps * 32, 0, st>>>(c->hits, c->hcnt, n, cap, row_cap, A.T, c->tau);
         ++launches;
     }

@@ -102,3 +102,24 @@ def test_dynamic_list_is_symmetric_at_scale(ctx):
     bwd = ge.astype(np.int64) * n + src
     assert np.array_equal(np.sort(fwd), np.sort(bwd))
     assert np.all(ge[gi] >= 0) and cnt.min() >= 1  # self is always present
+
+
+@pytest.mark.parametrize("tag", ["h0125", "h00625", "h012"])
+@pytest.mark.parametrize("cap", [0, 4])
+def test_golden_pairs_decided_like_the_reference(ctx, tag, cap):
+    # pairs within a few ulps of |a - b| = h, decided by the reference's own
+    # compiled Vector3f::norm (tests/golden/ref_math.npz): each pair is
+    # isolated, so a particle's list is itself plus its partner iff d < h
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_math.npz"))
+    pairs, d, h = g["pairs_" + tag], g["norm_" + tag][:, 0], float(g["h_" + tag])
+    x = pairs.reshape(-1, 3)
+    hi = tuple(float(v) for v in x.max(0) + 0.1)
+    gi, ge, _ = gpu_query(ctx, x, h, (0.0, 0.0, 0.0), hi, cap)
+    got = rows(gi, ge, cap, x.shape[0])
+    n = pairs.shape[0]
+    want_pair = d < np.float32(h)
+    bad = [k for k in range(n)
+           if sorted(got[2 * k].tolist()) != ([2 * k, 2 * k + 1] if want_pair[k] else [2 * k])
+           or sorted(got[2 * k + 1].tolist()) != ([2 * k, 2 * k + 1] if want_pair[k] else [2 * k + 1])]
+    assert not bad, f"{len(bad)} of {n} pairs decided differently, first {bad[:5]}"
