@@ -42,6 +42,10 @@ def pbd_bytes_per_particle_step(kbar, iters):
     return 176.0 + 4.0 * kbar + iters * (44.0 + 8.0 * kbar)
 
 
+WORKLOAD = ("dam_break_2m: 128^3 jittered lattice, spacing 0.0025, radius 0.00625, cap 64, "
+            "5 Jacobi iterations, dt 5e-4, box 2x1x1")
+
+
 def pass_bytes(kind, kbar, kunion):
     """Algorithmic bytes per particle of one launch of a solver pass."""
     if kind == "density":  # read x_i, the N(i) row, write lambda
@@ -172,7 +176,8 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": n / v * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": "dam_break_2m sample", "particles": n, "cap": 64, "iterations": 5},
+        "config": {"workload": WORKLOAD, "particles": 2097152, "sample_particles": n, "cap": 64,
+                   "iterations": 5},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -288,8 +293,7 @@ def run_pk(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "dam_break_2m: 128^3 jittered lattice, spacing 0.0025, radius 0.00625, "
-                               "cap 64, 5 Jacobi iterations, dt 5e-4, box 2x1x1",
+        "config": {"workload": WORKLOAD,
                    "particles": n, "kbar": kbar, "solver_row_mean": kunion,
                    "solver_row_max": kmax, "iterations": sc.iterations,
                    "parallelism": "replicas" if world > 1 else "single",
