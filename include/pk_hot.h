@@ -137,6 +137,22 @@ int pk_advect(pk_ctx* ctx, float* x, const float* v, int n, float dt, pk_stream 
 int pk_update_velocity(pk_ctx* ctx, float* v, const float* x, const float* x_old, int n,
                        float dt, pk_stream stream);
 
+/* ---------------------------------------------------------- FixedPoints */
+
+/* FixedPoints::constrain (Dynamics/ParticleSystem/FixedPoints.cu:110-147,
+ * K_DoFixPoints :126-140): for k < count, x[ids[k]] = target[k] and
+ * v[ids[k]] = 0, as the reference's pins; with vel != NULL, v[ids[k]] = vel[k]
+ * instead (a pin moved kinematically, e.g. a pulled end; no reference
+ * counterpart).  ids outside [0, n) are skipped and reported as PK_ERR_ARG by
+ * pk_ctx_status.  target and vel are 3 floats per pin (device memory). */
+int pk_fixed_points(pk_ctx* ctx, float* x, float* v, int n, const int* ids, const float* target,
+                    const float* vel, int count, pk_stream stream);
+
+/* FixedPoints::constrainPositionToPlane (FixedPoints.cu:150-169): particles
+ * behind the plane through `origin` with unit normal `dir` are moved onto it. */
+int pk_plane_constrain(pk_ctx* ctx, float* x, int n, const float origin[3], const float dir[3],
+                       pk_stream stream);
+
 /* ------------------------------------------------- BoundaryConstraint */
 
 /* BoundaryConstraint::setCube (Dynamics/ParticleSystem/BoundaryConstraint.cu:108-117):
@@ -177,6 +193,21 @@ typedef struct {
  * allocation-free once the context has seen `n` (capturable in a CUDA graph). */
 int pk_pbf_step(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p,
                 float* rho_out, pk_stream stream);
+
+/* Many independent scenes in one frame (no reference counterpart; the
+ * reference steps each ParticleFluid node with its own launches).  The scenes'
+ * particles are concatenated in caller order: scene s owns particles
+ * [scene_offsets[s], scene_offsets[s+1]) of x, v and rho_out, with
+ * scene_offsets a device array of nscenes + 1 ints (0 first, n last,
+ * non-decreasing).  Every scene has its own box of the same geometry
+ * (p->nq.lo/hi, the context's boundary box) and the same parameters; scenes
+ * never interact.  The result for each scene is that of pk_pbf_step on that
+ * scene alone (the boundary jitter is seeded by the id within the scene).
+ * All scenes run in the same ~21 launches, asynchronous and allocation-free
+ * once the context has seen n and nscenes, so a frame can be captured in a
+ * CUDA graph. */
+int pk_pbf_step_batched(pk_ctx* ctx, float* x, float* v, const int* scene_offsets, int nscenes, int n,
+                        const pk_pbf_params* p, float* rho_out, pk_stream stream);
 
 /* Number of kernel launches the last pk_pbf_step enqueued. */
 int pk_last_launch_count(const pk_ctx* ctx);

@@ -474,10 +474,39 @@ void pko_sdf_constrain(int n, float* x, float* v, const pko_sdf* s, const float*
 #define real float
 #define SFX(name) name##_f
 #define RSQRT sqrtf
+#define FMA fmaf
 #include "pk_oracle_solver.inc"
 #undef real
 #undef SFX
 #undef RSQRT
+#undef FMA
+
+/* FixedPoints (FixedPoints.cu:126-162): pins and the plane constraint. */
+void pko_fixed_points(int n, float* x, float* v, const int* ids, const float* target, const float* vel,
+                      int count)
+{
+    int k, a;
+    for (k = 0; k < count; k++) {
+        const int i = ids[k];
+        if (i < 0 || i >= n) continue;
+        for (a = 0; a < 3; a++) {
+            x[3 * i + a] = target[3 * k + a];
+            v[3 * i + a] = vel ? vel[3 * k + a] : 0.0f;
+        }
+    }
+}
+
+void pko_plane_constrain(int n, float* x, const float origin[3], const float dir[3])
+{
+    int i, a;
+    for (i = 0; i < n; i++) {
+        const float ex = x[3 * i] - origin[0], ey = x[3 * i + 1] - origin[1], ez = x[3 * i + 2] - origin[2];
+        /* glm dot as nvcc fuses it: fma(z, z', fma(x, x', y*y')) */
+        const float tmp = fmaf(dir[2], ez, fmaf(dir[0], ex, dir[1] * ey));
+        if (tmp < 0.0f)
+            for (a = 0; a < 3; a++) x[3 * i + a] = fmaf(-tmp, dir[a], x[3 * i + a]);
+    }
+}
 
 /* The float kernel functions the solver uses, for checking against the
  * reference's compiled SpikyKernel / SmoothKernel / CorrectedKernel. */
@@ -496,6 +525,7 @@ void pko_kernels_f(int n, const float* r, float h, float* out5)
 #define real double
 #define SFX(name) name##_d
 #define RSQRT sqrt
+#define FMA fma
 #include "pk_oracle_solver.inc"
 #undef real
 #undef SFX

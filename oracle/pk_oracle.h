@@ -54,6 +54,12 @@ void  pko_grid_setup(pko_grid* g, float h, const float lo[3], const float hi[3])
 void  pko_set_norm_variant(int v);
 int   pko_get_norm_variant(void);
 float pko_dist3(const float* a, const float* b);
+/* FixedPoints::constrain (FixedPoints.cu:110-147): x[ids[k]] = target[k],
+ * v[ids[k]] = vel ? vel[k] : 0; ids outside [0, n) skipped. */
+void pko_fixed_points(int n, float* x, float* v, const int* ids, const float* target, const float* vel,
+                      int count);
+/* FixedPoints::constrainPositionToPlane (FixedPoints.cu:150-169). */
+void pko_plane_constrain(int n, float* x, const float origin[3], const float dir[3]);
 /* SpikyKernel Weight/Gradient, SmoothKernel::Weight, CorrectedKernel
  * Weight/WeightRR (Kernel.h:29-142) at radii r[n], float: out5[5*i + k]. */
 void  pko_kernels_f(int n, const float* r, float h, float* out5);
@@ -112,7 +118,9 @@ void pko_pd_inverse_k##sfx(int n, const int* index, int cap, long long total,   
 void pko_pd_solve##sfx(int n, real* x, real* v, const int* index, int cap, long long total,  \
                        const int* rest_idx, const real* rest_pos, const unsigned char* alive,\
                        const real* invK, const real* bulk, real horizon, real mu,            \
-                       real lambda, int iterations, real dt);
+                       real lambda, int iterations, real dt);                           \
+void pko_pd_break##sfx(int n, const real* x, const int* index, int cap, long long total,     \
+                       const int* rest_idx, const real* rest_pos, unsigned char* alive, real s);
 
 PKO_DECLARE(float, _f)
 PKO_DECLARE(double, _d)

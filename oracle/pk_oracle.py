@@ -33,6 +33,8 @@ def lib():
         L.pko_dist3.argtypes = [_f32p, _f32p]
         L.pko_dist3.restype = c_float
         L.pko_kernels_f.argtypes = [c_int, _f32p, c_float, _f32p]
+        L.pko_fixed_points.argtypes = [c_int, _f32p, _f32p, _i32p, _f32p, ctypes.c_void_p, c_int]
+        L.pko_plane_constrain.argtypes = [c_int, _f32p, _f32p, _f32p]
         L.pko_neighbor_query.argtypes = [c_int, _f32p, c_float, _f32p, _f32p, c_int,
                                          ctypes.c_void_p, ctypes.c_void_p, c_ll,
                                          ctypes.POINTER(c_ll)]
@@ -51,6 +53,8 @@ def lib():
                 c_int, rp, _i32p, _i32p, c_int, c_ll, _i32p, rp]
             getattr(L, "pko_pd_inverse_k" + sfx).argtypes = [
                 c_int, _i32p, c_int, c_ll, rp, rt, rp]
+            getattr(L, "pko_pd_break" + sfx).argtypes = [
+                c_int, rp, _i32p, c_int, c_ll, _i32p, rp, _u8p, rt]
             getattr(L, "pko_pd_solve" + sfx).argtypes = [
                 c_int, rp, rp, _i32p, c_int, c_ll, _i32p, rp, ctypes.c_void_p, rp, rp,
                 rt, rt, rt, c_int, rt]
@@ -94,6 +98,23 @@ def kernels(r, h):
     out = np.zeros((r.shape[0], 5), np.float32)
     lib().pko_kernels_f(r.shape[0], r, float(h), out)
     return out
+
+
+def fixed_points(x, v, ids, target, vel=None):
+    x = np.array(x, np.float32, copy=True)
+    v = np.array(v, np.float32, copy=True)
+    ids = np.ascontiguousarray(ids, np.int32)
+    target = np.ascontiguousarray(target, np.float32)
+    velp = None if vel is None else np.ascontiguousarray(vel, np.float32)
+    lib().pko_fixed_points(x.shape[0], x, v, ids, target,
+                           None if velp is None else velp.ctypes.data_as(ctypes.c_void_p), ids.shape[0])
+    return x, v
+
+
+def plane_constrain(x, origin, direction):
+    x = np.array(x, np.float32, copy=True)
+    lib().pko_plane_constrain(x.shape[0], x, _v3(origin), _v3(direction))
+    return x
 
 
 def _v3(a):
@@ -222,6 +243,16 @@ def pd_inverse_k(index, cap, total, rest_pos, h, dtype=np.float32):
         n, np.ascontiguousarray(index, np.int32), cap, total,
         np.ascontiguousarray(rest_pos, dt_), h, invK)
     return invK[: 9 * n].reshape(n, 3, 3)
+
+
+def pd_break(x, index, cap, total, rest_idx, rest_pos, alive, s, dtype=np.float32):
+    """Stretch break (mirrors the library's k_pd_break); updates `alive` in place."""
+    sfx, dt_ = _rt(dtype)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    getattr(lib(), "pko_pd_break" + sfx)(
+        x.shape[0] // 3, x, np.ascontiguousarray(index, np.int32), cap, total,
+        np.ascontiguousarray(rest_idx, np.int32), np.ascontiguousarray(rest_pos, dt_), alive, s)
+    return alive
 
 
 def pd_solve(x, v, index, cap, total, rest_idx, rest_pos, invK, bulk, horizon, mu, lam,

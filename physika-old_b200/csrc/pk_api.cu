@@ -268,6 +268,10 @@ PK_API int pk_ctx_status(pk_ctx* c, pk_stream stream)
     if (bits) {
         cudaMemset(c->d_err, 0, sizeof(int));
         char msg[160];
+        if (bits & pk::kErrBadIndex) {
+            snprintf(msg, sizeof msg, "a particle id outside [0, n) was given (flags 0x%x)", bits);
+            return fail(c, PK_ERR_ARG, msg);
+        }
         snprintf(msg, sizeof msg, "capacity exceeded on the device (flags 0x%x: 1=row, 2=hits>512, 4=list)", bits);
         return fail(c, PK_ERR_CAPACITY, msg);
     }
@@ -459,6 +463,27 @@ PK_API int pk_advect(pk_ctx* c, float* x, const float* v, int n, float dt, pk_st
     return check_launch(c, "pk_advect");
 }
 
+PK_API int pk_fixed_points(pk_ctx* c, float* x, float* v, int n, const int* ids, const float* target,
+                           const float* vel, int count, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || count < 0 || (count > 0 && (!x || !v || !ids || !target)))
+        return fail(c, PK_ERR_ARG, "bad positions, velocities, ids or targets");
+    cudaSetDevice(c->device);
+    c->launches = pk::fix_points(x, v, n, ids, target, vel, count, c->d_err, (cudaStream_t)stream);
+    return check_launch(c, "pk_fixed_points");
+}
+
+PK_API int pk_plane_constrain(pk_ctx* c, float* x, int n, const float origin[3], const float dir[3],
+                              pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || (n > 0 && !x) || !origin || !dir) return fail(c, PK_ERR_ARG, "bad arguments");
+    cudaSetDevice(c->device);
+    c->launches = pk::plane_constrain(x, n, origin, dir, (cudaStream_t)stream);
+    return check_launch(c, "pk_plane_constrain");
+}
+
 PK_API int pk_update_velocity(pk_ctx* c, float* v, const float* x, const float* x_old, int n, float dt,
                               pk_stream stream)
 {
@@ -622,8 +647,12 @@ PK_API int pk_boundary_jitter(pk_ctx* c, int n, float* out, pk_stream stream)
 // ======================================================================
 // fused fluid step
 
-PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, float* rho_out,
-                       pk_stream stream)
+namespace {
+
+// One frame for one scene, or for several scenes concatenated in caller order
+// (scene_off: device offsets, nscenes + 1 entries) that share the parameters.
+int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, float* rho_out,
+                  const int* scene_off, int nscenes, pk_stream stream, const char* what)
 {
     if (!c) return PK_ERR_ARG;
     if (!p) return fail(c, PK_ERR_ARG, "null step parameters");
@@ -636,6 +665,13 @@ PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params
     cudaSetDevice(c->device);
     cudaStream_t st = (cudaStream_t)stream;
     pk::Grid g = pk::make_grid(p->nq.radius, p->nq.lo, p->nq.hi);
+    if (nscenes > 1) {
+        if ((long long)nscenes * g.scene_keys > (1LL << 30))
+            return fail(c, PK_ERR_ARG, "scenes x cells per scene exceeds 2^30 keys");
+        g.nscenes = nscenes;
+        g.scene_off = scene_off;
+        g.nkeys = (long long)nscenes * g.scene_keys;
+    }
     const int row_cap = row_capacity(&p->nq);
     if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
         (rc = ensure_rows(c, (long long)n * row_cap)))
@@ -661,9 +697,26 @@ PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params
     l += pk::pbd_fast_solve(c, n, pk::make_spiky(p->pbd.smoothing_length), effective_mass(&p->pbd),
                             p->pbd.iterations, p->pbd.dt, x, v, rho_out, st);
     c->launches = l;
-    if ((rc = check_launch(c, "pk_pbf_step"))) return rc;
-    c->nq_valid = true;
+    if ((rc = check_launch(c, what))) return rc;
+    c->nq_valid = true;  // for batched scenes: the union of the scenes' lists
     return PK_OK;
+}
+
+}  // namespace
+
+PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, float* rho_out,
+                       pk_stream stream)
+{
+    return pbf_step_impl(c, x, v, n, p, rho_out, nullptr, 1, stream, "pk_pbf_step");
+}
+
+PK_API int pk_pbf_step_batched(pk_ctx* c, float* x, float* v, const int* scene_offsets, int nscenes,
+                               int n, const pk_pbf_params* p, float* rho_out, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (nscenes < 1 || (nscenes > 1 && !scene_offsets))
+        return fail(c, PK_ERR_ARG, "need at least one scene and its offsets");
+    return pbf_step_impl(c, x, v, n, p, rho_out, scene_offsets, nscenes, stream, "pk_pbf_step_batched");
 }
 
 // ======================================================================

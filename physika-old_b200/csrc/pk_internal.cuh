@@ -30,6 +30,7 @@ constexpr int kMaxHits = 512;  // per-particle hit buffer of the list build
 constexpr int kErrRowOverflow = 1;
 constexpr int kErrHitOverflow = 2;
 constexpr int kErrPublicOverflow = 4;
+constexpr int kErrBadIndex = 8;  // a particle id outside [0, n) (pins)
 
 // Uniform grid of the reference's GridHash (GridHash.cu:46-75): cell = radius,
 // two cells of padding.  Keys are blocked Morton: 4x4x4 cell blocks in
@@ -39,9 +40,30 @@ struct Grid {
     float ds;
     float lo[3];
     int nx, ny, nz;
-    int bx, by, bz;  // blocks per axis
-    long long nkeys; // bx*by*bz*64
+    int bx, by, bz;       // blocks per axis
+    long long nkeys;      // keys of all scenes: nscenes * scene_keys
+    long long scene_keys; // bx*by*bz*64, the keys of one scene's grid
+    int nscenes;          // scenes stepped together (1: a single scene)
+    const int* scene_off; // device, nscenes + 1 caller-order particle offsets (null when 1)
 };
+
+// Scene of caller particle i (0 for a single scene): scenes share one grid
+// geometry and each owns a disjoint key range [scene * scene_keys, ...), so no
+// particle ever meets another scene's particles.
+__device__ inline int scene_of(const Grid& g, int i)
+{
+    if (g.nscenes <= 1) return 0;
+    int lo = 0, hi = g.nscenes;  // scene_off[lo] <= i < scene_off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(g.scene_off + mid) <= i)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+__device__ inline int scene_key_base(const Grid& g, int i) { return (int)(scene_of(g, i) * g.scene_keys); }
 
 __host__ __device__ inline int morton2bit3(int i, int j, int k)
 {

@@ -41,6 +41,9 @@ int integrate_aos(float* x, float* v, const float* f, int n, const float g[3], f
                   cudaStream_t st);
 int advect_aos(float* x, const float* v, int n, float dt, cudaStream_t st);
 int velocity_from_positions(float* v, const float* x, const float* xold, int n, float dt, cudaStream_t st);
+int fix_points(float* x, float* v, int n, const int* ids, const float* target, const float* vel, int count,
+               int* err, cudaStream_t st);
+int plane_constrain(float* x, int n, const float origin[3], const float dir[3], cudaStream_t st);
 int boundary_aos(float* x, float* v, int n, const SdfView& s, float nfric, float tfric, float dt,
                  cudaStream_t st);
 SdfView sdf_view(const pk_ctx* c);

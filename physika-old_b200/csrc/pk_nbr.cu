@@ -151,14 +151,15 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
         const int2 rng = A.items[item];
         const float4 x0 = A.xs[rng.x];
         const int3 c = cell3(A.g, x0.x, x0.y, x0.z);
+        const int base = scene_key_base(A.g, __ldg(A.perm + rng.x));
         // the 27 neighbour ranges in one round: lane o < 27 owns offset o
         int beg = 0, len = 0;
         if (lane < 27) {
             const int key = cell_key(A.g, c.x + kOffset27[lane][0], c.y + kOffset27[lane][1],
                                      c.z + kOffset27[lane][2]);
             if (key >= 0) {
-                beg = __ldg(A.start + key);
-                len = __ldg(A.start + key + 1) - beg;
+                beg = __ldg(A.start + base + key);
+                len = __ldg(A.start + base + key + 1) - beg;
             }
         }
         int incl = len;

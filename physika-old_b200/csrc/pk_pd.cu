@@ -298,8 +298,10 @@ __global__ void __launch_bounds__(256)
         float r0 = rpos[3 * at] - rpos[3 * a0], r1 = rpos[3 * at + 1] - rpos[3 * a0 + 1],
               r2 = rpos[3 * at + 2] - rpos[3 * a0 + 2];
         float c0 = x[3 * j] - x[3 * i], c1 = x[3 * j + 1] - x[3 * i + 1], c2 = x[3 * j + 2] - x[3 * i + 2];
-        float lr = sqrtf(r0 * r0 + r1 * r1 + r2 * r2), lc = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
-        if (lc > (1.0f + s) * lr) alive[at] = 0;
+        // lengths rounded as Vector3f::norm compiles (fma(z,z,fma(x,x,y*y)))
+        float lr = __fsqrt_rn(__fmaf_rn(r2, r2, __fmaf_rn(r0, r0, __fmul_rn(r1, r1))));
+        float lc = __fsqrt_rn(__fmaf_rn(c2, c2, __fmaf_rn(c0, c0, __fmul_rn(c1, c1))));
+        if (lc > __fmul_rn(__fadd_rn(1.0f, s), lr)) alive[at] = 0;
     }
 }
 

@@ -32,7 +32,10 @@ Grid make_grid(float h, const float lo[3], const float hi[3])
     g.bx = (g.nx + 3) / 4;
     g.by = (g.ny + 3) / 4;
     g.bz = (g.nz + 3) / 4;
-    g.nkeys = (long long)g.bx * g.by * g.bz * 64;
+    g.scene_keys = (long long)g.bx * g.by * g.bz * 64;
+    g.nkeys = g.scene_keys;
+    g.nscenes = 1;
+    g.scene_off = nullptr;
     return g;
 }
 
@@ -59,16 +62,19 @@ __global__ void __launch_bounds__(256) k_keys(float* __restrict__ x, float* __re
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float3 p = make_float3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+    const int scene = scene_of(g, i);
     if (kBoundary) {
+        // the jitter is seeded by the particle's id within its own scene
+        const int local = g.nscenes > 1 ? i - __ldg(g.scene_off + scene) : i;
         float3 u = make_float3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
-        if (sdf_constrain(sdf, i, p, u, nfric, tfric, dt)) {
+        if (sdf_constrain(sdf, local, p, u, nfric, tfric, dt)) {
             x[3 * i] = p.x; x[3 * i + 1] = p.y; x[3 * i + 2] = p.z;
             v[3 * i] = u.x; v[3 * i + 1] = u.y; v[3 * i + 2] = u.z;
         }
     }
     int3 c = cell3(g, p.x, p.y, p.z);
     int k = cell_key(g, c.x, c.y, c.z);
-    if (k < 0) k = (int)g.nkeys;
+    k = k < 0 ? (int)g.nkeys : k + (int)(scene * g.scene_keys);
     key[i] = k;
     rank[i] = atomicAdd(&cell_cnt[k], 1);
 }

@@ -17,8 +17,9 @@ EXPORTED = [
     "pk_ctx_create", "pk_ctx_destroy", "pk_last_error", "pk_ctx_status", "pk_last_launch_count",
     "pk_ctx_profile", "pk_ctx_profile_read",
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
-    "pk_advect", "pk_update_velocity",
+    "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
+    "pk_pbf_step_batched",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
     "pk_noalloc_max_particles", "pk_pbd_solve_noalloc",
 ]
@@ -79,10 +80,13 @@ def load():
         "pk_integrate": ([P, P, P, P, I, ctypes.POINTER(F * 3), F, P], I),
         "pk_advect": ([P, P, P, I, F, P], I),
         "pk_update_velocity": ([P, P, P, P, I, F, P], I),
+        "pk_fixed_points": ([P, P, P, I, P, P, P, I, P], I),
+        "pk_plane_constrain": ([P, P, I, ctypes.POINTER(F * 3), ctypes.POINTER(F * 3), P], I),
         "pk_boundary_set_box": ([P, ctypes.POINTER(F * 3), ctypes.POINTER(F * 3), F, I, P], I),
         "pk_boundary_constrain": ([P, P, P, I, F, F, F, P], I),
         "pk_boundary_jitter": ([P, I, P, P], I),
         "pk_pbf_step": ([P, P, P, I, ctypes.POINTER(PbfParams), P, P], I),
+        "pk_pbf_step_batched": ([P, P, P, P, I, I, ctypes.POINTER(PbfParams), P, P], I),
         "pk_pd_init": ([P, P, I, P, P, I, LL, F, P], I),
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
@@ -234,6 +238,23 @@ class Context:
         self._check(self.L.pk_integrate(self.h, _ptr(x), _ptr(v), _ptr(f), x.shape[0],
                                         ctypes.byref(_f3(gravity)), float(dt), _stream()))
 
+    def advect(self, x, v, dt):
+        self._check(self.L.pk_advect(self.h, _ptr(x), _ptr(v), x.shape[0], float(dt), _stream()))
+
+    def update_velocity(self, v, x, x_old, dt):
+        self._check(self.L.pk_update_velocity(self.h, _ptr(v), _ptr(x), _ptr(x_old), x.shape[0],
+                                              float(dt), _stream()))
+
+    # ---- FixedPoints
+    def fixed_points(self, x, v, ids, target, vel=None):
+        """x[ids[k]] = target[k]; v[ids[k]] = vel[k] (or 0). ids int32, target/vel (count, 3)."""
+        self._check(self.L.pk_fixed_points(self.h, _ptr(x), _ptr(v), x.shape[0], _ptr(ids), _ptr(target),
+                                           _ptr(vel), ids.shape[0], _stream()))
+
+    def plane_constrain(self, x, origin, direction):
+        self._check(self.L.pk_plane_constrain(self.h, _ptr(x), x.shape[0], ctypes.byref(_f3(origin)),
+                                              ctypes.byref(_f3(direction)), _stream()))
+
     # ---- boundary
     def boundary_set_box(self, lo, hi, spacing, inverted=True):
         self._check(self.L.pk_boundary_set_box(self.h, ctypes.byref(_f3(lo)), ctypes.byref(_f3(hi)),
@@ -254,6 +275,12 @@ class Context:
     def pbf_step(self, x, v, params, rho_out=None):
         self._check(self.L.pk_pbf_step(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(params),
                                        _ptr(rho_out), _stream()))
+
+    def pbf_step_batched(self, x, v, scene_offsets, params, rho_out=None):
+        """One frame of len(scene_offsets) - 1 independent scenes concatenated in x, v."""
+        self._check(self.L.pk_pbf_step_batched(self.h, _ptr(x), _ptr(v), _ptr(scene_offsets),
+                                               scene_offsets.shape[0] - 1, x.shape[0],
+                                               ctypes.byref(params), _ptr(rho_out), _stream()))
 
     # ---- ElasticityModule
     def pd_init(self, x, index, elements, cap, total, horizon):

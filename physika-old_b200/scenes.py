@@ -87,3 +87,36 @@ def elastic_bar(seed=0, dims=(256, 64, 32), spacing=0.004, cap=80, stiffness=(0.
     return ElasticScene("elastic_bar", x, np.zeros_like(x), dims, spacing, 3.0 * spacing,
                         (0.0, 0.0, 0.0), tuple(float(e) for e in ext), cap, 1e-3, bulk=bulk,
                         break_stretch=0.02, steps=steps)
+
+
+@dataclass
+class BatchedScenes:
+    name: str
+    scenes: list             # FluidScene per scene (the configuration-0 parameters)
+    x: np.ndarray            # (sum n_s, 3) float32, scenes concatenated
+    v: np.ndarray
+    offsets: np.ndarray      # (nscenes + 1,) int32
+
+
+def batched_mix(seed=0, nscenes=256, n_min=1024, n_max=65536):
+    """nscenes independent dam-break blocks, particle counts log-uniform in
+    [n_min, n_max] (PCG64 seed), each a jittered lattice of about that many
+    particles (dims a x a x c, a = round(n^(1/3))) in its own unit box with the
+    32k dam break's parameters (spacing 0.005, radius 0.0125, cap 60, dt 1e-3,
+    5 Jacobi iterations)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    target = np.round(np.exp(rng.uniform(np.log(n_min), np.log(n_max), nscenes))).astype(np.int64)
+    scenes_, xs = [], []
+    for s, n in enumerate(target):
+        a = max(1, int(round(n ** (1.0 / 3.0))))
+        c = max(1, int(round(n / (a * a))))
+        base = dam_break_small(seed=seed * 100003 + s + 1, n_side=1)
+        x = lattice(a, a, c, base.spacing, 0.1, seed * 100003 + s + 1)
+        sc = FluidScene(f"scene{s}", x, np.zeros_like(x), base.spacing, base.radius, base.lo, base.hi,
+                        base.cap, base.dt, steps=100)
+        scenes_.append(sc)
+        xs.append(x)
+    counts = np.array([q.x.shape[0] for q in scenes_], np.int64)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    x = np.concatenate(xs).astype(np.float32)
+    return BatchedScenes(f"batched_{nscenes}", scenes_, x, np.zeros_like(x), offsets)
