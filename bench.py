@@ -196,6 +196,89 @@ def load_traffic():
     return {}
 
 
+BATCHED_WORKLOAD = ("256 independent dam-break scenes, particle counts log-uniform in [1024, 65536] "
+                    "(PCG64 seed 0), each a jittered lattice block in its own unit box with the 32k "
+                    "dam break's parameters (spacing 0.005, radius 0.0125, cap 60, dt 1e-3, 5 iterations)")
+
+
+def measure_batched(local, steps, warmup, barrier):
+    """The batched frame (one pk_pbf_step_batched for all scenes, also replayed
+    as a CUDA graph) against per-scene plain frames (one pk_pbf_step per scene),
+    same scenes, same GPU, device time with CUDA events."""
+    import torch
+    import pkhot
+
+    dev = torch.device("cuda", local)
+    b = scenes.batched_mix(seed=0)
+    sc0 = b.scenes[0]
+    n = int(b.offsets[-1])
+    ctx = pkhot.Context(local)
+    ctx.boundary_set_box(sc0.lo, sc0.hi, sc0.sdf_spacing, True)
+    prm = pkhot.pbf_params(pkhot.nq_params(sc0.radius, sc0.lo, sc0.hi, sc0.cap),
+                           pkhot.pbd_params(sc0.radius, sc0.spacing, sc0.rest_density, sc0.iterations,
+                                            sc0.dt), sc0.gravity, boundary=True)
+    x = torch.from_numpy(b.x.copy()).to(dev)
+    v = torch.zeros_like(x)
+    off = torch.from_numpy(b.offsets.astype(np.int32)).to(dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(torch.cuda.current_stream())
+        for _ in range(k):
+            fn()
+        e1.record(torch.cuda.current_stream())
+        barrier()
+        return e0.elapsed_time(e1) / k
+
+    for _ in range(warmup):
+        ctx.pbf_step_batched(x, v, off, prm)
+    ctx.check_status()
+    launches = ctx.launch_count()
+    ms_eager = timed(lambda: ctx.pbf_step_batched(x, v, off, prm), steps)
+    graph_ms, graph_note = None, None
+    try:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            ctx.pbf_step_batched(x, v, off, prm)
+        g.replay()
+        ms_graph = timed(g.replay, steps)
+        graph_ms = ms_graph
+        del g
+    except Exception as exc:  # the eager number still stands
+        graph_note = f"capture failed: {exc}"
+    ctx.check_status()
+    lo, hi = b.offsets[:-1], b.offsets[1:]
+    views = [(x[a:c], v[a:c]) for a, c in zip(lo, hi)]
+
+    def plain_frame():
+        for xs, vs in views:
+            ctx.pbf_step(xs, vs, prm)
+
+    plain_frame()
+    ctx.check_status()
+    ms_plain = timed(plain_frame, max(2, min(steps, 5)))
+    ctx.check_status()
+    ctx.close()
+    del stream
+
+    def entry(ms):
+        return {"value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms}
+
+    out = {"workload": BATCHED_WORKLOAD, "scenes": len(b.scenes), "particles": n,
+           "batched_eager": entry(ms_eager), "plain_per_scene": entry(ms_plain),
+           "launches_per_frame": {"batched": launches, "plain": launches * len(b.scenes)},
+           "speedup_vs_plain": ms_plain / ms_eager}
+    if graph_ms is not None:
+        out["batched_graph"] = entry(graph_ms)
+        out["speedup_vs_plain"] = ms_plain / min(graph_ms, ms_eager)
+    else:
+        out["batched_graph"] = None
+        out["graph_note"] = graph_note
+    return out
+
+
 def run_pk(args):
     import torch
     import torch.distributed as dist
@@ -309,12 +392,14 @@ def run_pk(args):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    ctx.close()
+    if not args.no_batched:
+        line["batched"] = measure_batched(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier)
     if rank == 0 and world == 1 and not args.no_cpu:
         cv, cores, cn = time_cpu(steps=2, warmup=1)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"2 steps of a {cn}-particle block with the 2M scene's "
                                           "parameters, CPU restatement, OpenMP"}
-    ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -330,6 +415,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="pk", choices=["pk", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes comparison")
     ap.add_argument("--side", type=int, default=128,
                     help="lattice side of the scene (128 = the 2,097,152-particle workload; "
                          "smaller sides are for profiling captures only)")
