@@ -260,6 +260,39 @@ int pk_pd_solve(pk_ctx* ctx, float* x, float* v, int n, const pk_pd_params* p,
 int pk_pd_get_rest_shape(pk_ctx* ctx, int* rest_idx, float* rest_pos, float* inv_k,
                          pk_stream stream);
 
+/* ------------------------------- differentiable peridynamics rollouts */
+
+/* No reference counterpart.  `steps` elasticity steps on the rest shape of
+ * pk_pd_init, each: v += dt*gravity, x += dt*v (ParticleIntegrator with no
+ * force), then ElasticityModule::solveElasticity as in pk_pd_solve (the
+ * projection's bond terms are gathered over each particle's outgoing and
+ * incoming bonds, so a replay repeats the forward bit for bit).  x, v (n AoS)
+ * in place; stiffness from pk_pd_set_bulk; break_stretch must be 0.  With
+ * checkpoint_every > 0 the state at every checkpoint_every-th step is kept in
+ * the context for pk_pd_rollout_backward. */
+int pk_pd_rollout(pk_ctx* ctx, float* x, float* v, int n, const float gravity[3], const pk_pd_params* p,
+                  int steps, int checkpoint_every, pk_stream stream);
+
+/* Reverse mode of the last checkpointed pk_pd_rollout: given dL/dx_T (xbar)
+ * and dL/dv_T (vbar, may be NULL), writes dL/dx_0, dL/dv_0 (n AoS) and
+ * dL/dbulk (n doubles: the stiffness gradient is accumulated in double).  The
+ * rollout is replayed segment by segment from its checkpoints, every
+ * projection iterate of a segment is kept, and each iteration is reversed by
+ * hand-written adjoint kernels.  The reverse state and its arithmetic are
+ * double (the float iterates are read as given): the adjoint differences
+ * neighbouring values, which float arithmetic does not carry over hundreds of
+ * projection iterations. */
+int pk_pd_rollout_backward(pk_ctx* ctx, const float* xbar, const float* vbar, float* grad_x0, float* grad_v0,
+                           double* grad_bulk, pk_stream stream);
+
+/* The same rollout and reverse mode in double precision (x, v, bulk doubles;
+ * the rest shape and K^-1 of pk_pd_init as given): the reference against which
+ * the float gradients and central finite differences are checked. */
+int pk_pd_rollout_f64(pk_ctx* ctx, double* x, double* v, const double* bulk, int n, const double gravity[3],
+                      const pk_pd_params* p, int steps, int checkpoint_every, pk_stream stream);
+int pk_pd_rollout_backward_f64(pk_ctx* ctx, const double* xbar, const double* vbar, double* grad_x0,
+                               double* grad_v0, double* grad_bulk, pk_stream stream);
+
 /* ------------------------------------------- DensityPBD without allocation */
 
 /* No counterpart in the reference.  For callers that may not allocate device

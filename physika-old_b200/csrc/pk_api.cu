@@ -242,7 +242,9 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->hcnt, c->items, c->nitems,
                     c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
-                    c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w};
+                    c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
+                    c->pd_in_cnt, c->pd_in_off, c->pd_in};
+    pk::pd_work_release(c);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& ev : c->prof_ev)
@@ -736,7 +738,8 @@ PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const 
     if (n > c->pd_cap_n) {
         size_t m = (size_t)n;
         if (!(regrow(c->pd_index, m) && regrow(c->pd_invK, 9 * m) && regrow(c->pd_bulk, m) &&
-              regrow(c->pd_xold, 3 * m) && regrow(c->pd_delta, 3 * m) && regrow(c->pd_w, m))) {
+              regrow(c->pd_xold, 3 * m) && regrow(c->pd_delta, 3 * m) && regrow(c->pd_w, m) &&
+              regrow(c->pd_in_cnt, m + 1) && regrow(c->pd_in_off, m + 1))) {
             c->pd_cap_n = 0;
             return fail(c, PK_ERR_NOMEM, "device allocation of elasticity state failed");
         }
@@ -744,7 +747,7 @@ PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const 
     }
     if (bonds > c->pd_cap_bonds) {
         if (!(regrow(c->pd_rest_idx, (size_t)bonds) && regrow(c->pd_rest_pos, 3 * (size_t)bonds) &&
-              regrow(c->pd_alive, (size_t)bonds))) {
+              regrow(c->pd_alive, (size_t)bonds) && regrow(c->pd_in, (size_t)bonds))) {
             c->pd_cap_bonds = 0;
             return fail(c, PK_ERR_NOMEM, "device allocation of the rest shape failed");
         }
@@ -754,7 +757,17 @@ PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const 
     c->pd_cap = cap;
     c->pd_total = bonds;
     c->pd_horizon = horizon;
+    if (bonds > (1LL << 31) - 1) return fail(c, PK_ERR_ARG, "more than 2^31 bonds");
+    long long parts = pk::scan_parts_needed(n + 1);
+    if (parts > c->cap_part) {
+        if (!regrow(c->scan_part, (size_t)parts)) {
+            c->cap_part = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of scan partials failed");
+        }
+        c->cap_part = parts;
+    }
     pk::pd_rest_shape(c, x, n, index, elements, cap, bonds, horizon, (cudaStream_t)stream);
+    if (n > 0) pk::pd_build_incoming(c, (cudaStream_t)stream);
     return check_launch(c, "pk_pd_init");
 }
 
@@ -782,7 +795,79 @@ PK_API int pk_pd_solve(pk_ctx* c, float* x, float* v, int n, const pk_pd_params*
     cudaSetDevice(c->device);
     c->launches = pk::pd_solve(c, x, v, n, p->horizon, p->mu, p->lambda, p->iterations, p->dt,
                                p->break_stretch, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_NOMEM, "device allocation of the projection workspace failed");
     return check_launch(c, "pk_pd_solve");
+}
+
+namespace {
+int check_rollout(pk_ctx* c, int n, const void* x, const void* v, const pk_pd_params* p, int steps, int every)
+{
+    if (!p) return fail(c, PK_ERR_ARG, "null elasticity parameters");
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    if (n != c->pd_n) return fail(c, PK_ERR_ARG, "particle count differs from pk_pd_init");
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    if (!(p->horizon > 0.0f) || !(p->dt > 0.0f) || p->iterations < 0 || steps < 0 || every < 0)
+        return fail(c, PK_ERR_ARG, "bad horizon, dt, iterations, steps or checkpoint interval");
+    if (p->break_stretch > 0.0f)
+        return fail(c, PK_ERR_ARG, "bond breaking is not differentiable: break_stretch must be 0 in a rollout");
+    return PK_OK;
+}
+}  // namespace
+
+PK_API int pk_pd_rollout(pk_ctx* c, float* x, float* v, int n, const float gravity[3], const pk_pd_params* p,
+                         int steps, int checkpoint_every, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_rollout(c, n, x, v, p, steps, checkpoint_every);
+    if (rc) return rc;
+    if (!gravity) return fail(c, PK_ERR_ARG, "null gravity");
+    cudaSetDevice(c->device);
+    c->pd_horizon_last = p->horizon;
+    c->pd_mu_last = p->mu;
+    c->pd_lambda_last = p->lambda;
+    c->launches = pk::pd_rollout_f32(c, x, v, n, gravity, p, steps, checkpoint_every, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_NOMEM, "device allocation of the rollout state failed");
+    return check_launch(c, "pk_pd_rollout");
+}
+
+PK_API int pk_pd_rollout_backward(pk_ctx* c, const float* xbar, const float* vbar, float* grad_x0, float* grad_v0,
+                                  double* grad_bulk, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n > 0 && (!xbar || !grad_x0 || !grad_v0 || !grad_bulk))
+        return fail(c, PK_ERR_ARG, "null adjoint or gradient arrays");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_backward_f32(c, xbar, vbar, grad_x0, grad_v0, grad_bulk, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_STATE, "no checkpointed float rollout to differentiate");
+    return check_launch(c, "pk_pd_rollout_backward");
+}
+
+PK_API int pk_pd_rollout_f64(pk_ctx* c, double* x, double* v, const double* bulk, int n, const double gravity[3],
+                             const pk_pd_params* p, int steps, int checkpoint_every, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_rollout(c, n, x, v, p, steps, checkpoint_every);
+    if (rc) return rc;
+    if (!gravity || (n > 0 && !bulk)) return fail(c, PK_ERR_ARG, "null gravity or bulk");
+    cudaSetDevice(c->device);
+    c->pd_horizon_last = p->horizon;
+    c->pd_mu_last = p->mu;
+    c->pd_lambda_last = p->lambda;
+    c->launches = pk::pd_rollout_f64(c, x, v, bulk, n, gravity, p, steps, checkpoint_every, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_NOMEM, "device allocation of the rollout state failed");
+    return check_launch(c, "pk_pd_rollout_f64");
+}
+
+PK_API int pk_pd_rollout_backward_f64(pk_ctx* c, const double* xbar, const double* vbar, double* grad_x0,
+                                      double* grad_v0, double* grad_bulk, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n > 0 && (!xbar || !grad_x0 || !grad_v0 || !grad_bulk))
+        return fail(c, PK_ERR_ARG, "null adjoint or gradient arrays");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_backward_f64(c, xbar, vbar, grad_x0, grad_v0, grad_bulk, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_STATE, "no checkpointed double rollout to differentiate");
+    return check_launch(c, "pk_pd_rollout_backward_f64");
 }
 
 PK_API int pk_pd_get_rest_shape(pk_ctx* c, int* rest_idx, float* rest_pos, float* inv_k, pk_stream stream)

@@ -93,4 +93,11 @@ struct pk_ctx {
     float pd_horizon = 0.0f;
     long long pd_cap_bonds = 0;
     int pd_cap_n = 0;
+    int* pd_in_cnt = nullptr;   // incoming bonds per particle (n + 1)
+    int* pd_in_off = nullptr;   // their CSR offsets (n + 1)
+    int2* pd_in = nullptr;      // (source particle, bond slot) of every incoming bond
+    // projection workspaces (float, double) and the parameters of the last rollout
+    void* pd_work32 = nullptr;
+    void* pd_work64 = nullptr;
+    float pd_horizon_last = 0.f, pd_mu_last = 0.f, pd_lambda_last = 0.f;
 };

@@ -49,6 +49,20 @@ int boundary_aos(float* x, float* v, int n, const SdfView& s, float nfric, float
 SdfView sdf_view(const pk_ctx* c);
 int boundary_jitter(float* out, int n, cudaStream_t st);
 
+// pk_pd_adj.cu
+int pd_build_incoming(pk_ctx* c, cudaStream_t st);
+int pd_project_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, float lambda, int iterations,
+                     float dt, cudaStream_t st);
+int pd_rollout_f32(pk_ctx* c, float* x, float* v, int n, const float g[3], const pk_pd_params* p, int steps,
+                   int every, cudaStream_t st);
+int pd_rollout_f64(pk_ctx* c, double* x, double* v, const double* bulk, int n, const double g[3],
+                   const pk_pd_params* p, int steps, int every, cudaStream_t st);
+int pd_backward_f32(pk_ctx* c, const float* xbar, const float* vbar, float* gx, float* gv, double* gbulk,
+                    cudaStream_t st);
+int pd_backward_f64(pk_ctx* c, const double* xbar, const double* vbar, double* gx, double* gv, double* gbulk,
+                    cudaStream_t st);
+void pd_work_release(pk_ctx* c);
+
 // pk_pd.cu
 int pd_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int* elements,
                   int cap, long long total, float horizon, cudaStream_t st);

@@ -6,19 +6,9 @@
 // (solveElasticity -> computeInverseK, :404-411).  Each projection iteration
 // is EM_EnforceElasticity (:123-242) + K_UpdatePosition (:281-292).
 #include "pk_kernels.cuh"
+#include "pk_pd_common.cuh"
 
 namespace pk {
-
-__device__ __forceinline__ int pd_size(const int* index, int cap, long long total, int n, int i)
-{
-    if (cap > 0) return index[i];
-    if (i >= n - 1) return (int)(total - index[i]);
-    return index[i + 1] - index[i];
-}
-__device__ __forceinline__ long long pd_at(const int* index, int cap, int i, int k)
-{
-    return cap > 0 ? (long long)cap * i + k : (long long)index[i] + k;
-}
 
 // K_UpdateRestShape (ElasticityModule.cu:449-494): copy the list, self to slot 0.
 __global__ void __launch_bounds__(256)
@@ -49,23 +39,6 @@ __global__ void __launch_bounds__(256)
             rpos[3 * a0 + 2] = x[3 * j + 2];
         }
     }
-}
-
-// CorrectedKernel / SmoothKernel (Kernel.h:68-75,99-142).
-__device__ __forceinline__ float smooth_w(float r, float h)
-{
-    float q = r / h;
-    return q > 1.0f ? 0.0f : (1.0f - q * q);
-}
-__device__ __forceinline__ float corr_w(float r, float h)
-{
-    float q = r / h;
-    return q * q * q * smooth_w(r, h);
-}
-__device__ __forceinline__ float corr_wrr(float r, float h)
-{
-    float q = r / h;
-    return q * smooth_w(r, h) / (h * h);
 }
 
 // Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations in double.
@@ -160,126 +133,6 @@ __global__ void __launch_bounds__(256) k_fill_u8(unsigned char* __restrict__ p, 
     if (t < m) p[t] = v;
 }
 
-__device__ __forceinline__ void normalize_or_zero(float& a, float& b, float& c)
-{
-    // v.norm() > EPSILON ? v.normalize() : 0 (ElasticityModule.cu:211-212);
-    // normalize() is 0 below FLT_EPSILON (vector_3d.inl:220-224).
-    float l = sqrtf(a * a + b * b + c * c);
-    if (l > kEpsilon && l > 1.1920928955078125e-7f) {
-        float is = 1.0f / l;
-        a *= is; b *= is; c *= is;
-    } else {
-        a = b = c = 0.f;
-    }
-}
-
-// EM_EnforceElasticity (ElasticityModule.cu:123-242); `alive` masks broken bonds.
-__global__ void __launch_bounds__(128)
-    k_pd_enforce(const float* __restrict__ x, int n, const int* __restrict__ index, int cap,
-                 long long total, const int* __restrict__ ridx, const float* __restrict__ rpos,
-                 const unsigned char* __restrict__ alive, const float* __restrict__ invK,
-                 const float* __restrict__ bulk, float horizon, float mu, float lambda,
-                 float* __restrict__ delta, float* __restrict__ wts)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    long long a0 = pd_at(index, cap, i, 0);
-    const float ri0 = rpos[3 * a0], ri1 = rpos[3 * a0 + 1], ri2 = rpos[3 * a0 + 2];
-    const float ci0 = x[3 * i], ci1 = x[3 * i + 1], ci2 = x[3 * i + 2];
-    const int m = pd_size(index, cap, total, n, i);
-    const float bulk_i = bulk[i];
-    float F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, tw = 0.f;
-    for (int e = 0; e < m; ++e) {
-        long long at = pd_at(index, cap, i, e);
-        if (!alive[at]) continue;
-        int j = ridx[at];
-        float e0 = rpos[3 * at] - ri0, e1 = rpos[3 * at + 1] - ri1, e2 = rpos[3 * at + 2] - ri2;
-        float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
-        if (r > kEpsilon) {
-            float wt = corr_w(r, horizon);
-            float p[3] = {(x[3 * j] - ci0) / horizon, (x[3 * j + 1] - ci1) / horizon,
-                          (x[3 * j + 2] - ci2) / horizon};
-            float q[3] = {e0 / horizon * wt, e1 / horizon * wt, e2 / horizon * wt};
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b) F[a][b] += p[a] * q[b];
-            tw += wt;
-        }
-    }
-    if (tw > kEpsilon) {
-        float s = 1.0f / tw, G[3][3];
-        const float* K = invK + 9LL * i;
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) F[a][b] *= s;
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) G[a][b] = F[a][0] * K[b] + F[a][1] * K[3 + b] + F[a][2] * K[6 + b];
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) F[a][b] = G[a][b];
-    }
-    float det = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
-                F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
-                F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
-    if (det < -0.001f) {
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) F[a][b] = (a == b) ? 1.f : 0.f;
-    }
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, accA = 0.f;
-    for (int e = 0; e < m; ++e) {
-        long long at = pd_at(index, cap, i, e);
-        if (!alive[at]) continue;
-        int j = ridx[at];
-        float e0 = ri0 - rpos[3 * at], e1 = ri1 - rpos[3 * at + 1], e2 = ri2 - rpos[3 * at + 2];
-        float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
-        if (!(r > 0.01f * horizon)) continue;
-        float xj0 = x[3 * j], xj1 = x[3 * j + 1], xj2 = x[3 * j + 2];
-        float rd0 = F[0][0] * e0 + F[0][1] * e1 + F[0][2] * e2;
-        float rd1 = F[1][0] * e0 + F[1][1] * e1 + F[1][2] * e2;
-        float rd2 = F[2][0] * e0 + F[2][1] * e1 + F[2][2] * e2;
-        float cd0 = ci0 - xj0, cd1 = ci1 - xj1, cd2 = ci2 - xj2;
-        normalize_or_zero(cd0, cd1, cd2);
-        normalize_or_zero(rd0, rd1, rd2);
-        float wrr = corr_wrr(r, horizon);
-        float mu_ij = mu * bulk_i * wrr, la_ij = lambda * bulk_i * wrr, dw = mu_ij + la_ij;
-        // mu/lambda targets for i (x_j + r*dir) and for j (x_i - r*dir)
-        float d0 = mu_ij * (xj0 + r * rd0) + la_ij * (xj0 + r * cd0);
-        float d1 = mu_ij * (xj1 + r * rd1) + la_ij * (xj1 + r * cd1);
-        float d2 = mu_ij * (xj2 + r * rd2) + la_ij * (xj2 + r * cd2);
-        float b0 = mu_ij * (ci0 - r * rd0) + la_ij * (ci0 - r * cd0);
-        float b1 = mu_ij * (ci1 - r * rd1) + la_ij * (ci1 - r * cd1);
-        float b2 = mu_ij * (ci2 - r * rd2) + la_ij * (ci2 - r * cd2);
-        accA += dw;
-        acc0 += d0; acc1 += d1; acc2 += d2;
-        atomicAdd(wts + j, dw);
-        atomicAdd(delta + 3 * j, b0);
-        atomicAdd(delta + 3 * j + 1, b1);
-        atomicAdd(delta + 3 * j + 2, b2);
-    }
-    atomicAdd(wts + i, accA);
-    atomicAdd(delta + 3 * i, acc0);
-    atomicAdd(delta + 3 * i + 1, acc1);
-    atomicAdd(delta + 3 * i + 2, acc2);
-}
-
-// K_UpdatePosition (ElasticityModule.cu:281-292): x = (x_old + delta)/(1 + w).
-__global__ void __launch_bounds__(256)
-    k_pd_update(float* __restrict__ x, const float* __restrict__ xold, const float* __restrict__ delta,
-                const float* __restrict__ wts, int n)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float den = 1.0f + wts[i];
-    x[3 * i] = (xold[3 * i] + delta[3 * i]) / den;
-    x[3 * i + 1] = (xold[3 * i + 1] + delta[3 * i + 1]) / den;
-    x[3 * i + 2] = (xold[3 * i + 2] + delta[3 * i + 2]) / den;
-}
-
-__global__ void __launch_bounds__(256)
-    k_pd_velocity(float* __restrict__ v, const float* __restrict__ x, const float* __restrict__ xold,
-                  long long m, float dt)
-{
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < m) v[t] += (x[t] - xold[t]) / dt;
-}
-
 // Stretch break (no reference counterpart): a bond dies for good once
 // |x_i - x_j| > (1 + s) * |rest_i - rest_j|.
 __global__ void __launch_bounds__(256)
@@ -325,26 +178,16 @@ int pd_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, floa
              int iterations, float dt, float break_stretch, cudaStream_t st)
 {
     if (n <= 0) return 0;
-    const unsigned nb = (unsigned)((n + 255) / 256), nb128 = (unsigned)((n + 127) / 128);
-    const long long m3 = 3LL * n;
     int launches = 0;
-    cudaMemcpyAsync(c->pd_xold, x, sizeof(float) * (size_t)m3, cudaMemcpyDeviceToDevice, st);
     if (break_stretch > 0.f) {
-        k_pd_break<<<nb, 256, 0, st>>>(x, n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_idx,
-                                       c->pd_rest_pos, c->pd_alive, break_stretch);
+        k_pd_break<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, c->pd_index, c->pd_cap, c->pd_total,
+                                                               c->pd_rest_idx, c->pd_rest_pos, c->pd_alive,
+                                                               break_stretch);
         ++launches;
     }
-    for (int it = 0; it < iterations; ++it) {
-        cudaMemsetAsync(c->pd_delta, 0, sizeof(float) * (size_t)m3, st);
-        cudaMemsetAsync(c->pd_w, 0, sizeof(float) * (size_t)n, st);
-        k_pd_enforce<<<nb128, 128, 0, st>>>(x, n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_idx,
-                                            c->pd_rest_pos, c->pd_alive, c->pd_invK, c->pd_bulk,
-                                            horizon, mu, lambda, c->pd_delta, c->pd_w);
-        k_pd_update<<<nb, 256, 0, st>>>(x, c->pd_xold, c->pd_delta, c->pd_w, n);
-        launches += 2;
-    }
-    k_pd_velocity<<<(unsigned)((m3 + 255) / 256), 256, 0, st>>>(v, x, c->pd_xold, m3, dt);
-    return launches + 1;
+    // the projection as gathers over outgoing and incoming bonds (pk_pd_adj.cu)
+    const int l = pd_project_solve(c, x, v, n, horizon, mu, lambda, iterations, dt, st);
+    return l < 0 ? l : launches + l;
 }
 
 }  // namespace pk

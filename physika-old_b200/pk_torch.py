@@ -1,0 +1,53 @@
+"""torch.autograd.Function over the peridynamics rollout of the C ABI.
+
+PdRollout.apply(x0, v0, bulk, ctx, settings) runs `steps` ElasticityModule
+steps (integration + projection) on the sm_100a library and returns x_T; its
+backward calls the hand-written adjoint (pk_pd_rollout_backward), which
+replays the rollout from checkpoints and returns dL/dx0, dL/dv0 and dL/dbulk.
+float32 and float64 tensors are supported (the float64 path is the reference
+for gradient checks).  The context must have been initialised with pd_init on
+the rest shape; bond breaking is not differentiable and is off.
+"""
+from dataclasses import dataclass
+
+import torch
+
+
+@dataclass
+class RolloutSettings:
+    horizon: float
+    mu: float = 0.05
+    lam: float = 0.1
+    iterations: int = 10
+    dt: float = 1e-3
+    steps: int = 200
+    checkpoint_every: int = 20
+    gravity: tuple = (0.0, -9.8, 0.0)
+
+
+class PdRollout(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, x0, v0, bulk, pk_ctx, s):
+        x = x0.detach().clone().contiguous()
+        v = v0.detach().clone().contiguous()
+        b = bulk.detach().contiguous()
+        if x.dtype == torch.float32:
+            pk_ctx.pd_set_bulk(b)
+            pk_ctx.pd_rollout(x, v, s.horizon, s.mu, s.lam, s.iterations, s.dt, s.steps, s.checkpoint_every,
+                              s.gravity)
+        else:
+            pk_ctx.pd_rollout(x, v, s.horizon, s.mu, s.lam, s.iterations, s.dt, s.steps, s.checkpoint_every,
+                              s.gravity, bulk64=b)
+        fctx.pk_ctx = pk_ctx
+        fctx.bulk_dtype = bulk.dtype
+        return x
+
+    @staticmethod
+    def backward(fctx, gx_t):
+        gx, gv, gb = fctx.pk_ctx.pd_rollout_backward(gx_t.contiguous())
+        return gx, gv, gb.to(fctx.bulk_dtype), None, None
+
+
+def pd_rollout(x0, v0, bulk, pk_ctx, settings):
+    """x_T of the rollout; differentiable in x0, v0 and bulk."""
+    return PdRollout.apply(x0, v0, bulk, pk_ctx, settings)

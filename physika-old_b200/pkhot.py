@@ -21,6 +21,7 @@ EXPORTED = [
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
     "pk_pbf_step_batched",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
+    "pk_pd_rollout", "pk_pd_rollout_backward", "pk_pd_rollout_f64", "pk_pd_rollout_backward_f64",
     "pk_noalloc_max_particles", "pk_pbd_solve_noalloc",
 ]
 
@@ -91,6 +92,11 @@ def load():
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
         "pk_pd_get_rest_shape": ([P, P, P, P, P], I),
+        "pk_pd_rollout": ([P, P, P, I, ctypes.POINTER(F * 3), ctypes.POINTER(PdParams), I, I, P], I),
+        "pk_pd_rollout_backward": ([P, P, P, P, P, P, P], I),
+        "pk_pd_rollout_f64": ([P, P, P, P, I, ctypes.POINTER(ctypes.c_double * 3), ctypes.POINTER(PdParams),
+                               I, I, P], I),
+        "pk_pd_rollout_backward_f64": ([P, P, P, P, P, P, P], I),
         "pk_noalloc_max_particles": ([], I),
         "pk_pbd_solve_noalloc": ([P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
     }
@@ -293,6 +299,32 @@ class Context:
     def pd_solve(self, x, v, horizon, mu=0.05, lam=0.1, iterations=10, dt=1e-3, break_stretch=0.0):
         p = PdParams(float(horizon), float(mu), float(lam), int(iterations), float(dt), float(break_stretch))
         self._check(self.L.pk_pd_solve(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(p), _stream()))
+
+    def pd_rollout(self, x, v, horizon, mu=0.05, lam=0.1, iterations=10, dt=1e-3, steps=1,
+                   checkpoint_every=0, gravity=(0.0, -9.8, 0.0), bulk64=None):
+        """`steps` peridynamics steps (integrate + projection) in place, keeping a
+        checkpoint every `checkpoint_every` steps for pd_rollout_backward.  x, v
+        float32 (bulk from pd_set_bulk) or float64 (then bulk64 is the stiffness)."""
+        import torch
+        p = PdParams(float(horizon), float(mu), float(lam), int(iterations), float(dt), 0.0)
+        if x.dtype == torch.float64:
+            g = (ctypes.c_double * 3)(*[float(a) for a in gravity])
+            self._check(self.L.pk_pd_rollout_f64(self.h, _ptr(x), _ptr(v), _ptr(bulk64), x.shape[0],
+                                                 ctypes.byref(g), ctypes.byref(p), int(steps),
+                                                 int(checkpoint_every), _stream()))
+        else:
+            self._check(self.L.pk_pd_rollout(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(_f3(gravity)),
+                                             ctypes.byref(p), int(steps), int(checkpoint_every), _stream()))
+
+    def pd_rollout_backward(self, xbar, vbar=None):
+        """Gradients (dL/dx0, dL/dv0, dL/dbulk) of the last checkpointed rollout of
+        xbar's precision, given dL/dx_T (and dL/dv_T)."""
+        import torch
+        gx, gv = torch.empty_like(xbar), torch.empty_like(xbar)
+        gb = torch.empty(xbar.shape[0], dtype=torch.float64, device=xbar.device)
+        fn = self.L.pk_pd_rollout_backward_f64 if xbar.dtype == torch.float64 else self.L.pk_pd_rollout_backward
+        self._check(fn(self.h, _ptr(xbar), _ptr(vbar), _ptr(gx), _ptr(gv), _ptr(gb), _stream()))
+        return gx, gv, gb
 
     def pd_get_rest_shape(self, rest_idx=None, rest_pos=None, inv_k=None):
         self._check(self.L.pk_pd_get_rest_shape(self.h, _ptr(rest_idx), _ptr(rest_pos), _ptr(inv_k),
