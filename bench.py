@@ -279,6 +279,168 @@ def measure_batched(local, steps, warmup, barrier):
     return out
 
 
+ADJOINT_WORKLOAD = ("differentiable rollout: 64x32x32 = 65,536-particle peridynamics block, spacing 0.004, "
+                    "horizon 3 spacing, cap 80, 10 projection iterations, dt 1e-3, 200 steps, checkpoint "
+                    "every 20; loss = mean |x_T - x_target|^2, target from hidden stiffness U[0.5, 2]e4 and "
+                    "v0 ~ N(0, 0.05^2) (PCG64 seeds 0, 1); guess: stiffness 1e4, v0 ~ N(0, 0.05^2) (seed 3)")
+PD_WORKLOAD = ("peridynamics bar 256x64x32 = 524,288 particles, spacing 0.004, horizon 3 spacing, cap 80, "
+               "stiffness U[0.8, 1.2]e4, 10 projection iterations, bonds break at 2% stretch, x-index 0 "
+               "clamped, last x layer pulled at 0.5 m/s, dt 1e-3")
+
+
+def pd_bytes_per_particle_step(kb, iters):
+    """Algorithmic HBM bytes of one peridynamics particle-step (bond indices read
+    per iteration, K^-1/bulk/x per particle; breaks: alive bits)."""
+    return 108.0 + iters * (108.0 + 4.0 * kb + kb / 8.0) + 4.0 * kb + kb / 8.0
+
+
+def measure_pd(local, steps, warmup, barrier):
+    """The elastic bar with fracture: integrate, pins, projection with stretch
+    break, pins; particle-steps/s over `steps` steps, device time."""
+    import torch
+    import pkhot
+
+    dev = torch.device("cuda", local)
+    sc = scenes.elastic_bar(seed=0)
+    n = sc.x.shape[0]
+    ctx = pkhot.Context(local)
+    x = torch.from_numpy(sc.x.copy()).to(dev)
+    v = torch.zeros_like(x)
+    idx, el, tot = ctx.nq_build(x, sc.horizon, sc.lo, sc.hi, sc.cap)
+    kb = float(idx.double().mean())
+    ctx.pd_init(x, idx, el, sc.cap, tot, sc.horizon)
+    ctx.pd_set_bulk(torch.from_numpy(sc.bulk).to(dev))
+    dims = sc.dims
+    ix = np.arange(n) // (dims[1] * dims[2])
+    left, right = np.nonzero(ix == 0)[0], np.nonzero(ix == dims[0] - 1)[0]
+    ids = torch.from_numpy(np.concatenate([left, right]).astype(np.int32)).to(dev)
+    base = x[ids.long()].clone()
+    vel = torch.zeros_like(base)
+    vel[left.shape[0]:, 0] = 0.5
+    step_no = [0]
+
+    def step():
+        step_no[0] += 1
+        tgt = base + vel * (step_no[0] * sc.dt)
+        ctx.integrate(x, v, (0.0, -9.8, 0.0), sc.dt)
+        ctx.fixed_points(x, v, ids, tgt, vel)
+        ctx.pd_solve(x, v, sc.horizon, sc.mu, sc.lam, sc.iterations, sc.dt, sc.break_stretch)
+        ctx.fixed_points(x, v, ids, tgt, vel)
+
+    for _ in range(warmup):
+        step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.current_stream())
+    for _ in range(steps):
+        step()
+    e1.record(torch.cuda.current_stream())
+    barrier()
+    ctx.check_status()
+    ms = e0.elapsed_time(e1) / steps
+    ctx.close()
+    peak, kind = peaks()
+    val = n / (ms / 1e3)
+    b = pd_bytes_per_particle_step(kb, sc.iterations)
+    return {"workload": PD_WORKLOAD, "particles": n, "value": val, "unit": UNIT, "ms_per_step": ms,
+            "steps": steps, "kbar_bonds": kb,
+            "step_roofline": {"bytes_per_particle_step": b, "frac": val * b / (peak * 1e9), "peak_source": kind}}
+
+
+def measure_adjoint(local, fd_coords=16):
+    """cfg4: float rollout with checkpoints, its reverse pass, and a check of
+    the double-precision adjoint against central differences of double rollouts."""
+    import torch
+    import pkhot
+
+    dev = torch.device("cuda", local)
+    sc = scenes.elastic_bar(seed=0, dims=(64, 32, 32), cap=80, stiffness=(0.5e4, 2.0e4))
+    n = sc.x.shape[0]
+    ctx = pkhot.Context(local)
+    x0 = torch.from_numpy(sc.x.copy()).to(dev)
+    idx, el, tot = ctx.nq_build(x0, sc.horizon, sc.lo, sc.hi, sc.cap)
+    ctx.pd_init(x0, idx, el, sc.cap, tot, sc.horizon)
+    steps, every = 200, 20
+    rng = np.random.Generator(np.random.PCG64(0))
+    bulk_true = rng.uniform(0.5e4, 2.0e4, n)
+    v_true = np.random.Generator(np.random.PCG64(1)).normal(0, 0.05, (n, 3))
+    args = (sc.horizon, sc.mu, sc.lam, sc.iterations, sc.dt)
+
+    def roll32(v, bulk, ck):
+        x = x0.clone()
+        vv = v.clone()
+        ctx.pd_set_bulk(bulk)
+        ctx.pd_rollout(x, vv, *args, steps, ck)
+        return x
+
+    target = roll32(torch.from_numpy(v_true.astype(np.float32)).to(dev),
+                    torch.from_numpy(bulk_true.astype(np.float32)).to(dev), 0)
+    # the initial guess: uniform stiffness, initial velocities from another draw
+    bulk = torch.full((n,), 1.0e4, dtype=torch.float32, device=dev)
+    v0 = torch.from_numpy(np.random.Generator(np.random.PCG64(3)).normal(0, 0.05, (n, 3))
+                          .astype(np.float32)).to(dev)
+    roll32(v0, bulk, every)  # warm-up (workspace allocation)
+    ctx.pd_rollout_backward(torch.ones_like(x0))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    xT = roll32(v0, bulk, every)
+    ev[1].record()
+    seed = 2.0 * (xT - target) / n
+    gx, gv, gb = ctx.pd_rollout_backward(seed)
+    ev[2].record()
+    torch.cuda.synchronize()
+    fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    loss32 = float(((xT - target) ** 2).sum(1).mean())
+
+    # double: adjoint gradient and central differences
+    x064, t64 = x0.double(), target.double()
+
+    def roll64(v, b, ck):
+        x = x064.clone()
+        vv = v.clone()
+        ctx.pd_rollout(x, vv, *args, steps, ck, bulk64=b)
+        return x
+
+    b64, v64 = bulk.double(), v0.double()
+    xT64 = roll64(v64, b64, every)
+    gx64, gv64, gb64 = ctx.pd_rollout_backward(2.0 * (xT64 - t64) / n)
+
+    def dL(vp, bp, vm, bm):
+        # L(+) - L(-) from the two trajectories, without subtracting two losses
+        xp, xm = roll64(vp, bp, 0), roll64(vm, bm, 0)
+        return float(((xp - xm) * (xp + xm - 2.0 * t64)).sum(1).mean())
+
+    pick = np.random.Generator(np.random.PCG64(2))
+    errs = {"bulk": [], "v0": []}
+    for k in pick.choice(n, fd_coords // 2, replace=False):
+        eps = 1e-4 * float(b64[k])
+        bp, bm = b64.clone(), b64.clone()
+        bp[k] += eps
+        bm[k] -= eps
+        fd = dL(v64, bp, v64, bm) / (2 * eps)
+        errs["bulk"].append(abs(fd - float(gb64[k])) / max(abs(fd), 1e-300))
+    for k in pick.choice(3 * n, fd_coords - fd_coords // 2, replace=False):
+        vp, vm = v64.clone(), v64.clone()
+        vp.view(-1)[k] += 1e-4
+        vm.view(-1)[k] -= 1e-4
+        fd = dL(vp, b64, vm, b64) / 2e-4
+        errs["v0"].append(abs(fd - float(gv64.view(-1)[k])) / max(abs(fd), 1e-300))
+    ctx.check_status()
+    rel32 = {"bulk": float((gb - gb64).norm() / gb64.norm()),
+             "v0": float((gv.double() - gv64).norm() / gv64.norm())}
+    ctx.close()
+    return {"workload": ADJOINT_WORKLOAD, "particles": n, "steps": steps, "checkpoint_every": every,
+            "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "forward_particle_steps_per_s": n * steps / (fwd / 1e3), "loss": loss32,
+            "fd_check": {"coords": {k: len(v) for k, v in errs.items()}, "eps": 1e-4,
+                         "eps_note": "relative for stiffness, absolute for velocity",
+                         "precision": "fp64, central differences from trajectory differences",
+                         "max_rel_err": {k: max(v) for k, v in errs.items()},
+                         "median_rel_err": {k: float(np.median(v)) for k, v in errs.items()}},
+            "fp32_vs_fp64_gradient_rel": rel32}
+
+
 def run_pk(args):
     import torch
     import torch.distributed as dist
@@ -395,6 +557,10 @@ def run_pk(args):
     ctx.close()
     if not args.no_batched:
         line["batched"] = measure_batched(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier)
+    if not args.no_pd:
+        line["peridynamics"] = measure_pd(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier)
+    if not args.no_adjoint:
+        line["adjoint"] = measure_adjoint(local)
     if rank == 0 and world == 1 and not args.no_cpu:
         cv, cores, cn = time_cpu(steps=2, warmup=1)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port",
@@ -416,6 +582,8 @@ def main():
     ap.add_argument("--impl", default="pk", choices=["pk", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes comparison")
+    ap.add_argument("--no-pd", action="store_true", help="skip the peridynamics bar")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable rollout")
     ap.add_argument("--side", type=int, default=128,
                     help="lattice side of the scene (128 = the 2,097,152-particle workload; "
                          "smaller sides are for profiling captures only)")

@@ -95,11 +95,44 @@ struct PdBonds {
     float h, mu, lambda;
 };
 
+// Every particle is handled by a group of kPdG lanes of one warp: lane `sub`
+// takes bonds sub, sub + kPdG, ... and the group's partial sums are combined
+// with xor shuffles in a fixed order (deterministic, so a replayed rollout
+// repeats the forward bit for bit).
+constexpr int kPdG = 8;
+constexpr int kPdBlock = 128;
+constexpr unsigned kPdAll = 0xffffffffu;
+
+template <class R>
+__device__ __forceinline__ R gsum(R v)
+{
+#pragma unroll
+    for (int o = kPdG / 2; o >= 1; o >>= 1) v += __shfl_xor_sync(kPdAll, v, o);
+    return v;
+}
+
+struct PdLane {
+    int i, sub;
+    bool valid;
+};
+__device__ __forceinline__ PdLane pd_lane(int n)
+{
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    PdLane L;
+    L.i = gid / kPdG;
+    L.sub = gid % kPdG;
+    L.valid = L.i < n;
+    if (!L.valid) L.i = n - 1;  // idle lanes of the last group mirror a valid particle, write nothing
+    return L;
+}
+
 // First loop of EM_EnforceElasticity: F_i = (sum p q^T / tw) K^-1 with
 // p = (x_j - x_i)/h, q = e wt / h, e = rest_j - rest_i, and the identity when
-// det F < -0.001.  Also returns tw and whether the identity was taken.
+// det F < -0.001.  Called by all lanes of i's group; every lane gets F, tw
+// and whether the identity was taken.
 template <class R, class RX>
-__device__ void pd_deformation(const PdBonds& B, const RX* x, int i, R F[3][3], float& tw_out, bool& ident)
+__device__ void pd_deformation(const PdBonds& B, const RX* x, int i, int sub, R F[3][3], float& tw_out,
+                               bool& ident)
 {
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
@@ -108,7 +141,7 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, R F[3][3], 
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) F[a][b] = 0;
     float tw = 0.f;
-    for (int e = 0; e < m; ++e) {
+    for (int e = sub; e < m; e += kPdG) {
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const int j = B.ridx[at];
@@ -124,6 +157,9 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, R F[3][3], 
             tw += wt;
         }
     }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) F[a][b] = gsum(F[a][b]);
+    tw = gsum(tw);
     if (tw > kEpsilon) {
         const R s = (R)1 / (R)tw;
         const float* K = B.invK + 9LL * i;
@@ -146,17 +182,22 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, R F[3][3], 
     tw_out = tw;
 }
 
+// F of every particle; with twout, also tw, stored negated when the identity
+// was taken (the reverse pass reads both instead of recomputing them).
 template <class R>
-__global__ void __launch_bounds__(128) k_pd_F(PdBonds B, const R* __restrict__ x, R* __restrict__ Fout)
+__global__ void __launch_bounds__(kPdBlock)
+    k_pd_F(PdBonds B, const R* __restrict__ x, R* __restrict__ Fout, float* __restrict__ twout)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n) return;
+    const PdLane L = pd_lane(B.n);
     R F[3][3];
     float tw;
     bool ident;
-    pd_deformation(B, x, i, F, tw, ident);
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) Fout[9LL * i + 3 * a + b] = F[a][b];
+    pd_deformation(B, x, L.i, L.sub, F, tw, ident);
+    if (L.valid && L.sub == 0) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) Fout[9LL * L.i + 3 * a + b] = F[a][b];
+        if (twout) twout[L.i] = ident ? -1.0f - tw : tw;
+    }
 }
 
 template <class R>
@@ -168,16 +209,16 @@ __device__ __forceinline__ V3<R> mat_e(const R* F, float e0, float e1, float e2)
 
 // W_i (the denominator of K_UpdatePosition): constant while bulk and the bonds are.
 template <class R, class RB>
-__global__ void __launch_bounds__(128) k_pd_W(PdBonds B, const RB* __restrict__ bulk, R* __restrict__ W)
+__global__ void __launch_bounds__(kPdBlock) k_pd_W(PdBonds B, const RB* __restrict__ bulk, R* __restrict__ W)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n) return;
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
     const int m = pd_size(B.index, B.cap, B.total, B.n, i);
     const R ml = (R)B.mu + (R)B.lambda;
     R w = 0;
-    for (int e = 0; e < m; ++e) {
+    for (int e = L.sub; e < m; e += kPdG) {
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
@@ -185,7 +226,7 @@ __global__ void __launch_bounds__(128) k_pd_W(PdBonds B, const RB* __restrict__ 
         if (!(r > 0.01f * B.h)) continue;
         w += ml * (R)bulk[i] * (R)corr_wrr(r, B.h);
     }
-    for (int t = B.in_off[i]; t < B.in_off[i + 1]; ++t) {
+    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
         const int2 kb = B.in_list[t];
         const long long at = kb.y;
         if (!B.alive[at]) continue;
@@ -196,24 +237,25 @@ __global__ void __launch_bounds__(128) k_pd_W(PdBonds B, const RB* __restrict__ 
         if (!(r > 0.01f * B.h)) continue;
         w += ml * (R)bulk[kb.x] * (R)corr_wrr(r, B.h);
     }
-    W[i] = w;
+    w = gsum(w);
+    if (L.valid && L.sub == 0) W[i] = w;
 }
 
 // One projection iteration: xn = (xold + D(x)) / (1 + W).
 template <class R>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPdBlock)
     k_pd_P(PdBonds B, const R* __restrict__ x, const R* __restrict__ xold, const R* __restrict__ F,
            const R* __restrict__ bulk, const R* __restrict__ W, R* __restrict__ xn)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n) return;
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
     const V3<R> ci = ld3(x, i);
     const int m = pd_size(B.index, B.cap, B.total, B.n, i);
     const R* Fi = F + 9LL * i;
     V3<R> acc{0, 0, 0};
-    for (int e = 0; e < m; ++e) {
+    for (int e = L.sub; e < m; e += kPdG) {
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
@@ -231,7 +273,7 @@ __global__ void __launch_bounds__(128)
         acc.y += mu * (dj.y + rr * nf.y) + la * (dj.y + rr * nc.y);
         acc.z += mu * (dj.z + rr * nf.z) + la * (dj.z + rr * nc.z);
     }
-    for (int t = B.in_off[i]; t < B.in_off[i + 1]; ++t) {
+    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
         const int2 kb = B.in_list[t];
         const long long at = kb.y;
         if (!B.alive[at]) continue;
@@ -253,6 +295,10 @@ __global__ void __launch_bounds__(128)
         acc.y += mu * (dk.y - rr * nf.y) + la * (dk.y - rr * nc.y);
         acc.z += mu * (dk.z - rr * nf.z) + la * (dk.z - rr * nc.z);
     }
+    acc.x = gsum(acc.x);
+    acc.y = gsum(acc.y);
+    acc.z = gsum(acc.z);
+    if (!L.valid || L.sub != 0) return;
     // (x_old + D)/(1 + W) written about x_i: the bond targets enter as offsets
     // from x_i, which keeps float accuracy at the scale of the bonds instead of
     // the scale of the coordinates
@@ -286,16 +332,20 @@ __global__ void __launch_bounds__(256)
 // Per source particle i: Fbar_i over its bonds, the bulk_i gradient, and
 // G_i = dL/dFraw_i / (tw h) (0 when the identity was taken).
 template <class R, class RX>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPdBlock)
     k_pd_adjB(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ xn, const RX* __restrict__ bulk,
-              const R* __restrict__ a, R* __restrict__ G, double* __restrict__ bulkbar)
+              const RX* __restrict__ Fst, const float* __restrict__ twst, const R* __restrict__ a,
+              R* __restrict__ G, double* __restrict__ bulkbar)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n) return;
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
+    // the forward's F of this iterate, and its tw (negated: identity taken)
     R F[3][3];
-    float tw;
-    bool ident;
-    pd_deformation<R, RX>(B, x, i, F, tw, ident);
+    for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) F[p][q] = (R)Fst[9LL * i + 3 * p + q];
+    const float tws = twst[i];
+    const bool ident = tws < 0.f;
+    const float tw = ident ? -1.0f - tws : tws;
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
     const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i), yi = ld3r<R>(xn, i);
@@ -303,7 +353,7 @@ __global__ void __launch_bounds__(128)
     const int m = pd_size(B.index, B.cap, B.total, B.n, i);
     R Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     R gb = 0;  // d L / d bulk_i
-    for (int e = 0; e < m; ++e) {
+    for (int e = L.sub; e < m; e += kPdG) {
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
@@ -334,6 +384,10 @@ __global__ void __launch_bounds__(128)
                       dot3(aj, V3<R>{ci.x - rr * nc.x - yj.x, ci.y - rr * nc.y - yj.y, ci.z - rr * nc.z - yj.z});
         gb += wrr * ((R)B.mu * tmu + (R)B.lambda * tla);
     }
+    for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) Fb[p][q] = gsum(Fb[p][q]);
+    gb = gsum(gb);
+    if (!L.valid || L.sub != 0) return;
     bulkbar[i] += (double)gb;
     R Gi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (!ident) {
@@ -356,12 +410,12 @@ __global__ void __launch_bounds__(128)
 
 // dL/dx_i for the input x of the iteration.
 template <class R, class RX>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPdBlock)
     k_pd_adjC(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ bulk, const R* __restrict__ a,
               const R* __restrict__ G, R* __restrict__ gout)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n) return;
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
     const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i);
@@ -370,7 +424,7 @@ __global__ void __launch_bounds__(128)
     const R* Gi = G + 9LL * i;
     const R ml = (R)B.mu + (R)B.lambda;
     V3<R> out{0, 0, 0};
-    for (int e = 0; e < m; ++e) {
+    for (int e = L.sub; e < m; e += kPdG) {
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const int j = B.ridx[at];
@@ -395,7 +449,7 @@ __global__ void __launch_bounds__(128)
         out.y += dw * aj.y + uc.y;
         out.z += dw * aj.z + uc.z;
     }
-    for (int t = B.in_off[i]; t < B.in_off[i + 1]; ++t) {
+    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
         const int2 kb = B.in_list[t];
         const long long at = kb.y;
         if (!B.alive[at]) continue;
@@ -424,6 +478,10 @@ __global__ void __launch_bounds__(128)
         out.y += dw * ak.y - uc.y;
         out.z += dw * ak.z - uc.z;
     }
+    out.x = gsum(out.x);
+    out.y = gsum(out.y);
+    out.z = gsum(out.z);
+    if (!L.valid || L.sub != 0) return;
     gout[3 * i] = out.x;
     gout[3 * i + 1] = out.y;
     gout[3 * i + 2] = out.z;
@@ -534,6 +592,8 @@ __global__ void __launch_bounds__(256) k_convert(long long m, const RI* __restri
 
 // ---------------------------------------------------------------- host side
 
+static unsigned pd_groups_blocks(int n) { return (unsigned)(((long long)n * kPdG + kPdBlock - 1) / kPdBlock); }
+
 // Forward state in R (float or double); the reverse state always in double:
 // the adjoint differences neighbouring values (a_i - a_j, x_i - x_j) and
 // sums over ~80 bonds per particle, 10 iterations per step, which float
@@ -553,6 +613,10 @@ struct PdWork {
     long long ckpt_cap = 0;
     R* seg = nullptr;   // iterates of one segment: every * (iterations + 1) * 3n
     long long seg_cap = 0;
+    R* segF = nullptr;  // F of every iterate of a segment: every * iterations * 9n
+    long long segF_cap = 0;
+    float* segT = nullptr;  // tw of every iterate (negated: identity taken)
+    long long segT_cap = 0;
 };
 
 template <class R>
@@ -595,7 +659,7 @@ static void work_free(PdWork<R>* w)
 {
     if (!w) return;
     void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->a, w->G, w->g, w->xoldbar,
-                  w->xb, w->vb, w->Wa, w->bulkbar, w->ckpt, w->seg};
+                  w->xb, w->vb, w->Wa, w->bulkbar, w->ckpt, w->seg, w->segF, w->segT};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete w;
@@ -670,14 +734,14 @@ template <class R>
 static int project(PdWork<R>& w, const PdBonds& B, R* x, const R* bulk, int iterations, cudaStream_t st)
 {
     const int n = B.n;
-    const unsigned nb128 = (unsigned)((n + 127) / 128);
+    const unsigned nb128 = pd_groups_blocks(n);
     const size_t bytes = sizeof(R) * 3 * (size_t)n;
     cudaMemcpyAsync(w.xold, x, bytes, cudaMemcpyDeviceToDevice, st);
     R* cur = x;
     R* nxt = w.xa;
     for (int it = 0; it < iterations; ++it) {
-        k_pd_F<R><<<nb128, 128, 0, st>>>(B, cur, w.F);
-        k_pd_P<R><<<nb128, 128, 0, st>>>(B, cur, w.xold, w.F, bulk, w.W, nxt);
+        k_pd_F<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.F, nullptr);
+        k_pd_P<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.xold, w.F, bulk, w.W, nxt);
         R* t = cur;
         cur = nxt;
         nxt = t;
@@ -693,7 +757,7 @@ int pd_project_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float 
     PdWork<float>* w = ensure_work<float>(c, n);
     if (!w) return -1;
     const PdBonds B = bonds_of(c, horizon, mu, lambda);
-    k_pd_W<float, float><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(B, c->pd_bulk, w->W);
+    k_pd_W<float, float><<<pd_groups_blocks(n), kPdBlock, 0, st>>>(B, c->pd_bulk, w->W);
     int l = 1 + project<float>(*w, B, x, c->pd_bulk, iterations, st);
     const long long m3 = 3LL * n;
     k_pd_vel<float><<<(unsigned)((m3 + 255) / 256), 256, 0, st>>>(m3, v, x, w->xold, dt);
@@ -704,6 +768,7 @@ template <class R>
 static int rollout(pk_ctx* c, R* x, R* v, const R* bulk_in, int n, const R g[3], const pk_pd_params* p, int steps,
                    int every, cudaStream_t st)
 {
+    if (n <= 0) return 0;
     PdWork<R>* w = ensure_work<R>(c, n);
     if (!w) return -1;
     const PdBonds B = bonds_of(c, p->horizon, p->mu, p->lambda);
@@ -713,6 +778,8 @@ static int rollout(pk_ctx* c, R* x, R* v, const R* bulk_in, int n, const R g[3],
     if (every > 0) {
         if (!grow(w->ckpt, w->ckpt_cap, 6LL * n * std::max(nseg, 1))) return -1;
         if (!grow(w->seg, w->seg_cap, 3LL * n * (p->iterations + 1) * every)) return -1;
+        if (!grow(w->segF, w->segF_cap, 9LL * n * std::max(p->iterations, 1) * every)) return -1;
+        if (!grow(w->segT, w->segT_cap, 1LL * n * std::max(p->iterations, 1) * every)) return -1;
     }
     w->steps = steps;
     w->every = every;
@@ -722,7 +789,7 @@ static int rollout(pk_ctx* c, R* x, R* v, const R* bulk_in, int n, const R g[3],
     for (int a = 0; a < 3; ++a) w->gravity[a] = g[a];
     const unsigned nb = (unsigned)((n + 255) / 256);
     const long long m3 = 3LL * n;
-    k_pd_W<R, R><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(B, w->bulk, w->W);
+    k_pd_W<R, R><<<pd_groups_blocks(n), kPdBlock, 0, st>>>(B, w->bulk, w->W);
     int l = 1;
     for (int s = 0; s < steps; ++s) {
         if (every > 0 && s % every == 0) {
@@ -742,19 +809,20 @@ template <class R>
 static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* gv, double* gbulk, cudaStream_t st)
 {
     PdWork<R>* w = work_of<R>(c);
+    if (c->pd_n == 0) return 0;
     if (!w || w->every <= 0 || w->n != c->pd_n) return -1;
     const int n = w->n, iters = w->iterations;
     const PdBonds B = bonds_of(c, c->pd_horizon_last, c->pd_mu_last, c->pd_lambda_last);
     const size_t bytes = sizeof(R) * 3 * (size_t)n;
     const long long m3 = 3LL * n;
-    const unsigned nb = (unsigned)((n + 255) / 256), nb128 = (unsigned)((n + 127) / 128),
+    const unsigned nb = (unsigned)((n + 255) / 256), nb128 = pd_groups_blocks(n),
                    nb3 = (unsigned)((m3 + 255) / 256);
     const R dt = (R)w->dt;
     k_convert<double, R><<<nb3, 256, 0, st>>>(m3, xbar, w->xb);
     k_convert<double, R><<<nb3, 256, 0, st>>>(m3, vbar, w->vb);
     cudaMemsetAsync(w->bulkbar, 0, sizeof(double) * (size_t)n, st);
-    k_pd_W<R, R><<<nb128, 128, 0, st>>>(B, w->bulk, w->W);
-    k_pd_W<double, R><<<nb128, 128, 0, st>>>(B, w->bulk, w->Wa);
+    k_pd_W<R, R><<<nb128, kPdBlock, 0, st>>>(B, w->bulk, w->W);
+    k_pd_W<double, R><<<nb128, kPdBlock, 0, st>>>(B, w->bulk, w->Wa);
     int l = 4;
     const int nseg = (w->steps + w->every - 1) / w->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
@@ -770,8 +838,10 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
             k_pd_integrate<R><<<nb, 256, 0, st>>>(n, xr, vr, w->gravity[0], w->gravity[1], w->gravity[2], dt);
             cudaMemcpyAsync(it, xr, bytes, cudaMemcpyDeviceToDevice, st);
             for (int k = 0; k < iters; ++k) {
-                k_pd_F<R><<<nb128, 128, 0, st>>>(B, it + 3LL * n * k, w->F);
-                k_pd_P<R><<<nb128, 128, 0, st>>>(B, it + 3LL * n * k, it, w->F, w->bulk, w->W, it + 3LL * n * (k + 1));
+                const long long slot = (long long)(s - s0) * iters + k;
+                R* Fk = w->segF + 9LL * n * slot;
+                k_pd_F<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, Fk, w->segT + 1LL * n * slot);
+                k_pd_P<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it, Fk, w->bulk, w->W, it + 3LL * n * (k + 1));
             }
             k_pd_vel<R><<<nb3, 256, 0, st>>>(m3, vr, it + 3LL * n * iters, it, dt);
             cudaMemcpyAsync(xr, it + 3LL * n * iters, bytes, cudaMemcpyDeviceToDevice, st);
@@ -782,9 +852,11 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
             k_pd_adj_head<double><<<nb3, 256, 0, st>>>(m3, w->xb, w->vb, (double)dt, w->g, w->xoldbar);
             for (int k = iters - 1; k >= 0; --k) {
                 k_pd_adjA<double><<<nb, 256, 0, st>>>(n, w->g, w->Wa, w->a, w->xoldbar);
-                k_pd_adjB<double, R><<<nb128, 128, 0, st>>>(B, it + 3LL * n * k, it + 3LL * n * (k + 1), w->bulk,
+                const long long slot = (long long)(s - s0) * iters + k;
+                k_pd_adjB<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it + 3LL * n * (k + 1), w->bulk,
+                                                             w->segF + 9LL * n * slot, w->segT + 1LL * n * slot,
                                                              w->a, w->G, w->bulkbar);
-                k_pd_adjC<double, R><<<nb128, 128, 0, st>>>(B, it + 3LL * n * k, w->bulk, w->a, w->G, w->g);
+                k_pd_adjC<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, w->bulk, w->a, w->G, w->g);
             }
             k_pd_adj_tail<double><<<nb3, 256, 0, st>>>(m3, w->g, w->xoldbar, (double)dt, w->xb, w->vb);
             l += 2 + 3 * iters;

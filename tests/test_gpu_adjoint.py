@@ -80,9 +80,11 @@ def test_adjoint_matches_finite_differences(ctx, oracle):
     loss.backward()
     gb, gv = bulk.grad.cpu().numpy(), v0.grad.cpu().numpy()
 
-    def L(b, v):
+    def dL(bp, vp, bm, vm):
+        # L(+) - L(-) from the two trajectories (no cancellation of two losses)
         with torch.no_grad():
-            return float(loss_fn(pd_rollout(x0, v, b, ctx, s), target))
+            xp, xm = pd_rollout(x0, vp, bp, ctx, s), pd_rollout(x0, vm, bm, ctx, s)
+            return float(((xp - xm) * (xp + xm - 2.0 * target)).sum(dim=1).mean())
 
     pick = np.random.default_rng(4)
     bad = []
@@ -91,7 +93,7 @@ def test_adjoint_matches_finite_differences(ctx, oracle):
         bp, bm = bulk.detach().clone(), bulk.detach().clone()
         bp[k] += eps
         bm[k] -= eps
-        fd = (L(bp, v0.detach()) - L(bm, v0.detach())) / (2 * eps)
+        fd = dL(bp, v0.detach(), bm, v0.detach()) / (2 * eps)
         if abs(fd - gb[k]) > 1e-3 * max(abs(fd), 1e-3 * np.abs(gb).max()):
             bad.append(("bulk", int(k), fd, gb[k]))
     for k in pick.choice(n * 3, 16, replace=False):
@@ -99,7 +101,7 @@ def test_adjoint_matches_finite_differences(ctx, oracle):
         vp, vm = v0.detach().clone(), v0.detach().clone()
         vp.view(-1)[k] += eps
         vm.view(-1)[k] -= eps
-        fd = (L(bulk.detach(), vp) - L(bulk.detach(), vm)) / (2 * eps)
+        fd = dL(bulk.detach(), vp, bulk.detach(), vm) / (2 * eps)
         g = gv.reshape(-1)[k]
         if abs(fd - g) > 1e-3 * max(abs(fd), 1e-3 * np.abs(gv).max()):
             bad.append(("v0", int(k), fd, g))
