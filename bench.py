@@ -201,16 +201,23 @@ BATCHED_WORKLOAD = ("256 independent dam-break scenes, particle counts log-unifo
                     "dam break's parameters (spacing 0.005, radius 0.0125, cap 60, dt 1e-3, 5 iterations)")
 
 
-def measure_batched(local, steps, warmup, barrier):
+def measure_batched(local, steps, warmup, barrier, max_over_ranks, rank, world):
     """The batched frame (one pk_pbf_step_batched for all scenes, also replayed
     as a CUDA graph) against per-scene plain frames (one pk_pbf_step per scene),
-    same scenes, same GPU, device time with CUDA events."""
+    same scenes, same GPU, device time with CUDA events.  With several ranks the
+    scenes are partitioned (largest first to the least-loaded rank) and each
+    rank steps its share; times are the max over ranks, values the whole job."""
     import torch
     import pkhot
+    from sharding import partition_scenes, subset
 
     dev = torch.device("cuda", local)
-    b = scenes.batched_mix(seed=0)
-    sc0 = b.scenes[0]
+    b_all = scenes.batched_mix(seed=0)
+    sc0 = b_all.scenes[0]
+    n_all = int(b_all.offsets[-1])
+    mine = partition_scenes(np.diff(b_all.offsets), world)[rank]
+    bx, bv, boff = subset(b_all.x, b_all.v, b_all.offsets, mine)
+    b = scenes.BatchedScenes(b_all.name, [b_all.scenes[s] for s in mine], bx, bv, boff)
     n = int(b.offsets[-1])
     ctx = pkhot.Context(local)
     ctx.boundary_set_box(sc0.lo, sc0.hi, sc0.sdf_spacing, True)
@@ -230,24 +237,27 @@ def measure_batched(local, steps, warmup, barrier):
             fn()
         e1.record(torch.cuda.current_stream())
         barrier()
-        return e0.elapsed_time(e1) / k
+        return max_over_ranks(e0.elapsed_time(e1) / k)
 
     for _ in range(warmup):
         ctx.pbf_step_batched(x, v, off, prm)
     ctx.check_status()
     launches = ctx.launch_count()
     ms_eager = timed(lambda: ctx.pbf_step_batched(x, v, off, prm), steps)
-    graph_ms, graph_note = None, None
+    graph_ms, graph_note, g = None, None, None
     try:
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             ctx.pbf_step_batched(x, v, off, prm)
         g.replay()
-        ms_graph = timed(g.replay, steps)
-        graph_ms = ms_graph
-        del g
     except Exception as exc:  # the eager number still stands
-        graph_note = f"capture failed: {exc}"
+        g, graph_note = None, f"capture failed: {exc}"
+    # every rank times the graph, or none does (the timing has collectives)
+    if max_over_ranks(0.0 if g is not None else 1.0) == 0.0:
+        graph_ms = timed(g.replay, steps)
+    elif graph_note is None:
+        graph_note = "capture failed on another rank"
+    g = None
     ctx.check_status()
     lo, hi = b.offsets[:-1], b.offsets[1:]
     views = [(x[a:c], v[a:c]) for a, c in zip(lo, hi)]
@@ -264,9 +274,10 @@ def measure_batched(local, steps, warmup, barrier):
     del stream
 
     def entry(ms):
-        return {"value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms}
+        return {"value": n_all / (ms / 1e3), "unit": UNIT, "ms_per_step": ms}
 
-    out = {"workload": BATCHED_WORKLOAD, "scenes": len(b.scenes), "particles": n,
+    out = {"workload": BATCHED_WORKLOAD, "scenes": len(b_all.scenes), "particles": n_all,
+           "scenes_per_rank": "largest-first greedy partition" if world > 1 else "all",
            "batched_eager": entry(ms_eager), "plain_per_scene": entry(ms_plain),
            "launches_per_frame": {"batched": launches, "plain": launches * len(b.scenes)},
            "speedup_vs_plain": ms_plain / ms_eager}
@@ -556,7 +567,8 @@ def run_pk(args):
     }
     ctx.close()
     if not args.no_batched:
-        line["batched"] = measure_batched(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier)
+        line["batched"] = measure_batched(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier,
+                                          max_over_ranks, rank, world)
     if not args.no_pd:
         line["peridynamics"] = measure_pd(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier)
     if not args.no_adjoint:
