@@ -139,7 +139,10 @@ __device__ __forceinline__ void sweep(const BuildArgs& A, const SweepSmem& S, in
 // of each 32-wide chunk of the 27 neighbour ranges: up to kPB independent
 // pair tests per lane and chunk, then one ballot per particle appends the
 // chunk's hits to its row (in candidate order, so rows are deterministic).
-__global__ void __launch_bounds__(kBuildWarps * 32) k_build(BuildArgs A)
+#ifndef PK_BUILD_MIN_BLOCKS
+#define PK_BUILD_MIN_BLOCKS 1  // resident blocks per SM asked of the register allocator
+#endif
+__global__ void __launch_bounds__(kBuildWarps * 32, PK_BUILD_MIN_BLOCKS) k_build(BuildArgs A)
 {
     extern __shared__ int smem_i[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -334,11 +337,51 @@ struct MemSrc {
     }
 };
 
+// Few keys above tau (E = c - cap small): tau is the (E+1)-th largest key.
+// Keys (d2 bits, index) pack into 64-bit integers whose order is the key
+// order; each lane sorts its <= 4 keys descending, then E+1 rounds take the
+// warp's largest head (two 32-bit warp maxima: d2, then index among equal d2)
+// and the owning lane advances.
+constexpr int kTopMax = 32;
+
+__device__ __forceinline__ void cswap_desc(unsigned long long& a, unsigned long long& b)
+{
+    const unsigned long long hi = a > b ? a : b, lo = a > b ? b : a;
+    a = hi;
+    b = lo;
+}
+
+// h: this lane's entries lane, lane+32, lane+64, lane+96 of the row (0 past c).
+__device__ __forceinline__ uint2 select_top(const uint2 (&h)[4], int E)
+{
+    unsigned long long k[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) k[q] = ((unsigned long long)h[q].y << 32) | h[q].x;
+    cswap_desc(k[0], k[1]);
+    cswap_desc(k[2], k[3]);
+    cswap_desc(k[0], k[2]);
+    cswap_desc(k[1], k[3]);
+    cswap_desc(k[1], k[2]);
+    unsigned md = 0u, mt = 0u;
+    for (int r = 0; r <= E; ++r) {
+        const unsigned hd = (unsigned)(k[0] >> 32), ht = (unsigned)k[0];
+        md = __reduce_max_sync(kFull, hd);
+        mt = __reduce_max_sync(kFull, hd == md ? ht : 0u);
+        if (hd == md && ht == mt) {
+            k[0] = k[1];
+            k[1] = k[2];
+            k[2] = k[3];
+            k[3] = 0ull;
+        }
+    }
+    return make_uint2(md, mt);
+}
+
 // A warp takes 32 consecutive particles: lane l reads the count of particle
 // base + l, the particles with more than cap hits are selected one after the
 // other (their rows loaded into registers when they hold at most 128 hits),
 // and lane l writes tau of particle base + l.
-__global__ void __launch_bounds__(kSelWarps * 32)
+__global__ void __launch_bounds__(kSelWarps * 32, 1)
     k_select(const uint2* __restrict__ hits, const int* __restrict__ hcnt, int n, int cap, int row_cap,
              float T, uint2* __restrict__ tau)
 {
@@ -352,18 +395,38 @@ __global__ void __launch_bounds__(kSelWarps * 32)
         const int c_l = s_l < n ? __ldg(hcnt + s_l) : 0;
         uint2 tau_l = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
         unsigned need = __ballot_sync(kFull, c_l > cap);
+        // rows of at most 128 hits are read into registers one particle ahead,
+        // so the next row's loads overlap the current selection
+        uint2 hn[4];
+        auto prefetch = [&](unsigned set, uint2(&h)[4]) {
+            const int q = set ? __ffs(set) - 1 : 0;
+            const int c = __shfl_sync(kFull, c_l, q);
+            const uint2* row = hits + (base + q) * row_cap;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int e = k * 32 + lane;
+                h[k] = (set && c <= 128 && e < c) ? __ldg(row + e) : make_uint2(0u, 0u);
+            }
+        };
+        prefetch(need, hn);
         while (need) {
             const int q = __ffs(need) - 1;
             need &= need - 1;
             const int c = __shfl_sync(kFull, c_l, q);
             const uint2* row = hits + (base + q) * row_cap;
+            uint2 h[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) h[k] = hn[k];
+            prefetch(need, hn);
             uint2 r;
-            if (c <= 32 * kSelRegChunks) {
+            if (c <= 32 * kSelRegChunks && c - cap + 1 <= kTopMax) {
+                r = select_top(h, c - cap);
+            } else if (c <= 32 * kSelRegChunks) {
                 RegSrc src;
 #pragma unroll
                 for (int k = 0; k < kSelRegChunks; ++k) {
                     const int e = k * 32 + lane;
-                    src.h[k] = e < c ? __ldg(row + e) : make_uint2(0u, 0xffffffffu);
+                    src.h[k] = e < c ? h[k] : make_uint2(0u, 0xffffffffu);
                 }
                 r = select_rank(src, (c + 31) / 32, row, c, cap - 1, T, S, lane, lt);
             } else {

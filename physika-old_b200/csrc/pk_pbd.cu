@@ -166,7 +166,10 @@ __global__ void __launch_bounds__(256)
     vs[s] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f);
 }
 
-constexpr int kGroup = 8;
+#ifndef PK_PASS_LANES
+#define PK_PASS_LANES 4  // lanes per particle in the Jacobi passes (measured at 2M: 4 < 8 < 16)
+#endif
+constexpr int kGroup = PK_PASS_LANES;
 
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
                    float* x, float* v, float* rho_out, cudaStream_t st)
