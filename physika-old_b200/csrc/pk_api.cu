@@ -331,7 +331,7 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
     pk::Grid g = pk::make_grid(p->radius, p->lo, p->hi);
     const int row_cap = row_capacity(p);
     if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
-        (rc = ensure_rows(c, (long long)n * row_cap)))
+        (rc = ensure_rows(c, pk::row_slots(n, row_cap))))
         return rc;
     c->nq_valid = false;
     c->grid = g;
@@ -676,7 +676,7 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     }
     const int row_cap = row_capacity(&p->nq);
     if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
-        (rc = ensure_rows(c, (long long)n * row_cap)))
+        (rc = ensure_rows(c, pk::row_slots(n, row_cap))))
         return rc;
     pk::SdfView sv{};
     if (p->boundary) sv = pk::sdf_view(c);

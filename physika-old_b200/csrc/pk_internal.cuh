@@ -26,6 +26,23 @@ constexpr int kRowFlagB = 1 << 30;
 constexpr int kRowIndexMask = (1 << 30) - 1;
 constexpr int kMaxHits = 512;  // per-particle hit buffer of the list build
 
+// Solver rows are interleaved by blocks of 32 sorted particles and quads of
+// entries: entries 4q .. 4q+3 of particle s are 16 contiguous bytes at
+// (((s / 32) * ceil(row_cap / 4) + q) * 32 + s % 32) * 4.  A warp whose lanes
+// walk their rows in step reads 512 contiguous bytes per quad (one 16-byte
+// load per lane), and at any entry index its lanes gather from a few
+// neighbour cells.  The array holds ceil(n / 32) * 32 * ceil(row_cap / 4) * 4
+// entries (row_slots).
+__host__ __device__ inline int row_quads(int row_cap) { return (row_cap + 3) >> 2; }
+__host__ __device__ inline long long row_slot(int s, int e, int row_cap)
+{
+    return (((long long)(s >> 5) * row_quads(row_cap) + (e >> 2)) * 32 + (s & 31)) * 4 + (e & 3);
+}
+__host__ __device__ inline long long row_slots(long long n, int row_cap)
+{
+    return ((n + 31) & ~31LL) * 4LL * row_quads(row_cap);
+}
+
 // Error bits latched in Ctx::d_err.
 constexpr int kErrRowOverflow = 1;
 constexpr int kErrHitOverflow = 2;

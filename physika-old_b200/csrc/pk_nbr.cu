@@ -466,8 +466,8 @@ __global__ void __launch_bounds__(256)
         ps = perm[s];
         if (pub) pbase = capped ? (long long)ps * cap : (long long)offs[ps];
     }
-    int* row = rows + (long long)(valid ? s : 0) * row_cap;
-    const uint2* hrow = hits + (long long)(valid ? s : 0) * row_cap;
+    const int so = valid ? s : 0;
+    const uint2* hrow = hits + (long long)so * row_cap;
     // every lane of the warp iterates to the longest row of the warp's groups
     int cmax = cnt;
 #pragma unroll
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(256)
         const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
         if (fa) {
             const int q = nA + __popc(ba & lt_g);
-            row[q] = t | kRowFlagA | (fb ? kRowFlagB : 0);
+            rows[row_slot(so, q, row_cap)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
             if (pub) {
                 const long long o = pbase + q;
                 if (capped ? (q < cap) : (o < pub_capacity))
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(256)
     __syncwarp();
     if (valid) {
         const int nBw = min(nB, kStash);
-        for (int e = sub; e < nBw; e += kEmitG) row[nA + e] = s_b[grp][e];
+        for (int e = sub; e < nBw; e += kEmitG) rows[row_slot(so, nA + e, row_cap)] = s_b[grp][e];
         if (sub == 0) {
             rcnt[s] = make_int2(nA, nA + nBw);
             if (pub_index != nullptr) pub_index[ps] = capped ? min(nA, cap) : offs[ps];

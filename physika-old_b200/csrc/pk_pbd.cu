@@ -10,22 +10,14 @@
 //           + [i in N(j)] -- the same sum the reference's scatter
 //           (+dp_ij to i, -dp_ij to j, DensityPBD.cu:134-179) accumulates,
 //           since dp_ji = -dp_ij bit for bit.
-// G lanes share one particle: each takes every G-th row entry, partial sums
-// are combined with xor shuffles.  Jacobi: pass A reads x, writes (x, lambda)
-// to xl; pass B reads xl only and writes x'.
+// One thread per particle walks its solver row; rows are interleaved by
+// blocks of 32 particles (row_slot), so a warp's row reads are one line per
+// entry and its gathers at one entry index touch a few neighbour cells.
+// Jacobi: pass A reads x, writes (x, lambda) to xl; pass B reads xl only and
+// writes x'.
 #include "pk_kernels.cuh"
 
 namespace pk {
-
-constexpr unsigned kAll = 0xffffffffu;
-
-template <int G>
-__device__ __forceinline__ float group_sum(float v)
-{
-#pragma unroll
-    for (int off = G / 2; off >= 1; off >>= 1) v += __shfl_xor_sync(kAll, v, off);
-    return v;
-}
 
 // Per-pair constants of the two passes (Spiky kernel, Kernel.h SpikyKernel).
 struct PassK {
@@ -48,34 +40,42 @@ __device__ __forceinline__ void pair_geom(float dx, float dy, float dz, float in
     dd = fmaxf(fmaf(-(d2 * ir), inv_h, 1.0f), 0.0f);
 }
 
-// Pass A: rho_i and lambda_i over N(i).  Writes xl[s] = (x_i, lambda_i) so
-// pass B gathers a neighbour's position and lambda in one 16-byte load.
-// sum |grad_j|^2 is taken as sum g_j^2 (|x_ij / r| = 1).
-template <int G>
+// One quad of row entries (16 bytes, streaming: the rows are read once per
+// pass and outgrow L2).
+__device__ __forceinline__ int4 row_quad(const int4* p) { return __ldcs(p); }
+
+// Pass A: rho_i and lambda_i over N(i), one thread per particle walking its
+// interleaved row.  Writes xl[s] = (x_i, lambda_i) so pass B gathers a
+// neighbour's position and lambda in one 16-byte load.  sum |grad_j|^2 is taken
+// as sum g_j^2 (|x_ij / r| = 1).
 __global__ void __launch_bounds__(256)
     k_pass_density(const float4* __restrict__ xs, const int* __restrict__ rows,
-                   const int2* __restrict__ rcnt, int row_cap, int n, PassK k,
+                   const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
                    float4* __restrict__ xl, float* __restrict__ rho_out)
 {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = gid / G, sub = gid % G;
-    const bool valid = s < n;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 xi = xs[s];
+    const int na = rcnt[s].x;
+    const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     float rho = 0.f, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid) {
-        xi = xs[s];
-        const int na = rcnt[s].x;
-        const int* row = rows + (long long)s * row_cap;
-#pragma unroll 2
-        for (int e = sub; e < na; e += G) {
-            const int j = __ldg(row + e) & kRowIndexMask;
+    const int nq = (na + 3) >> 2;
+    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    for (int q = 0; q < nq; ++q) {
+        const int4 cur = nxt;
+        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));  // next quad in flight
+        const int ent[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (4 * q + k >= na) break;
+            const int j = ent[k] & kRowIndexMask;
             const float4 xj = __ldg(xs + j);
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             float d2, ir, dd;
-            pair_geom(dx, dy, dz, k.inv_h, d2, ir, dd);
+            pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
             const float dd2 = dd * dd;
-            rho = fmaf(k.cwm, dd2 * dd, rho);
-            const float g = d2 > kEps2 ? k.cg * dd2 : 0.0f;
+            rho = fmaf(k_.cwm, dd2 * dd, rho);
+            const float g = d2 > kEps2 ? k_.cg * dd2 : 0.0f;
             const float gi = g * ir;
             gx = fmaf(gi, dx, gx);
             gy = fmaf(gi, dy, gy);
@@ -83,55 +83,48 @@ __global__ void __launch_bounds__(256)
             sg = fmaf(g, g, sg);
         }
     }
-    rho = group_sum<G>(rho);
-    sg = group_sum<G>(sg);
-    gx = group_sum<G>(gx);
-    gy = group_sum<G>(gy);
-    gz = group_sum<G>(gz);
-    if (valid && sub == 0) {
-        float l = sg + (gx * gx + gy * gy + gz * gz);
-        l = -(rho - 1000.0f) / (l + 0.1f);  // rest density hard-coded (DensityPBD.cu:87)
-        xl[s] = make_float4(xi.x, xi.y, xi.z, l > 0.0f ? 0.0f : l);
-        if (rho_out != nullptr) rho_out[s] = rho;
-    }
+    float l = sg + (gx * gx + gy * gy + gz * gz);
+    l = -(rho - 1000.0f) / (l + 0.1f);  // rest density hard-coded (DensityPBD.cu:87)
+    xl[s] = make_float4(xi.x, xi.y, xi.z, l > 0.0f ? 0.0f : l);
+    if (rho_out != nullptr) rho_out[s] = rho;
 }
 
 // Pass B: x_i' = x_i + sum over U(i) of m_ij * 10 (x_i - x_j)(lambda_i +
 // lambda_j) grad(r) / r (DensityPBD.cu:158), m_ij = popcount of the two flag
-// bits.
-template <int G>
+// bits; one thread per particle.
 __global__ void __launch_bounds__(256)
     k_pass_disp(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
-                int row_cap, int n, PassK k, float4* __restrict__ xs_out)
+                int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
 {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = gid / G, sub = gid % G;
-    const bool valid = s < n;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 xi = xl[s];
+    const int nu = rcnt[s].y;
+    const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     float ax = 0.f, ay = 0.f, az = 0.f;
-    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid) {
-        xi = xl[s];
-        const int nu = rcnt[s].y;
-        const int* row = rows + (long long)s * row_cap;
-#pragma unroll 2
-        for (int e = sub; e < nu; e += G) {
-            const int v = __ldg(row + e);
+    const int nq = (nu + 3) >> 2;
+    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    for (int q = 0; q < nq; ++q) {
+        const int4 cur = nxt;
+        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));  // next quad in flight
+        const int ent[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (4 * q + k >= nu) break;
+            const int v = ent[k];
             const int j = v & kRowIndexMask;
             const float mult = (float)__popc((unsigned)v >> 30);
             const float4 xj = __ldg(xl + j);
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             float d2, ir, dd;
-            pair_geom(dx, dy, dz, k.inv_h, d2, ir, dd);
-            const float c = d2 > kEps2 ? mult * (xi.w + xj.w) * (k.c10g * (dd * dd)) * ir : 0.0f;
+            pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
+            const float c = d2 > kEps2 ? mult * (xi.w + xj.w) * (k_.c10g * (dd * dd)) * ir : 0.0f;
             ax = fmaf(c, dx, ax);
             ay = fmaf(c, dy, ay);
             az = fmaf(c, dz, az);
         }
     }
-    ax = group_sum<G>(ax);
-    ay = group_sum<G>(ay);
-    az = group_sum<G>(az);
-    if (valid && sub == 0) xs_out[s] = make_float4(xi.x + ax, xi.y + ay, xi.z + az, 0.f);
+    xs_out[s] = make_float4(xi.x + ax, xi.y + ay, xi.z + az, 0.f);
 }
 
 // Sorted -> caller order: x, v += (x - x_old)/dt (DP_UpdateVelocity,
@@ -166,17 +159,11 @@ __global__ void __launch_bounds__(256)
     vs[s] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f);
 }
 
-#ifndef PK_PASS_LANES
-#define PK_PASS_LANES 4  // lanes per particle in the Jacobi passes (measured at 2M: 4 < 8 < 16)
-#endif
-constexpr int kGroup = PK_PASS_LANES;
-
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
                    float* x, float* v, float* rho_out, cudaStream_t st)
 {
     if (n <= 0) return 0;
     const unsigned nb1 = (unsigned)((n + 255) / 256);
-    const unsigned nbg = (unsigned)(((long long)n * kGroup + 255) / 256);
     int launches = 0;
     const float4* cur = c->xs0;
     const PassK pk = pass_k(k, mass);
@@ -185,11 +172,11 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     for (int it = 0; it < iterations; ++it) {
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
-        k_pass_density<kGroup><<<nbg, 256, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+        k_pass_density<<<nb1, 256, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
                                                     last ? c->rho : nullptr);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
-        k_pass_disp<kGroup><<<nbg, 256, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+        k_pass_disp<<<nb1, 256, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
         prof_end(c, PK_PROF_DISP, st);
         cur = c->xa;
         launches += 2;
