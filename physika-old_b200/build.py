@@ -36,6 +36,28 @@ def build_pkhot(force=False, verbose=True):
     return out
 
 
+def build_framework(force=False, verbose=True):
+    """The C++ Framework mirror (framework/*.cpp: the reference-named modules
+    and the headless scene driver) into lib/libpkframework.so, linked against
+    libpkhot.so (found next to it at run time)."""
+    out = os.path.join(HERE, "lib", "libpkframework.so")
+    fw = os.path.join(HERE, "framework")
+    srcs = [os.path.join(fw, s) for s in ("ParticleModules.cpp", "scene_driver.cpp")]
+    deps = srcs + glob.glob(os.path.join(fw, "*.h")) + [os.path.join(ROOT, "include", "pk_hot.h")]
+    if not force and not _newer(out, deps):
+        return out
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden", "-Wall",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"), *srcs,
+           "-L", os.path.join(HERE, "lib"), "-lpkhot", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(cuda, "lib64"), "-o", out + ".tmp"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(out + ".tmp", out)
+    return out
+
+
 REFERENCE = os.environ.get("PK_REFERENCE_SRC", "/root/reference")
 
 
@@ -52,4 +74,5 @@ def build_oracle(verbose=True, with_ref=False):
 
 if __name__ == "__main__":
     build_pkhot(force="--force" in sys.argv)
+    build_framework(force="--force" in sys.argv)
     build_oracle(with_ref=True)

@@ -159,6 +159,7 @@ public:
     typedef typename TDataType::Real Real;
     typedef typename TDataType::Coord Coord;
     BoundaryConstraint() = default;
+    using ConstraintModule::constrain;
     bool constrain(DeviceArray<Coord>& position, DeviceArray<Coord>& velocity, Real dt);
     void setCube(Coord lo, Coord hi, Real distance, bool inverted);
     Real m_normal_friction = 0.95f;

@@ -1,0 +1,86 @@
+"""The C++ Framework mirror (reference class names: ParticleFluid,
+PositionBasedFluidModel, NeighborQuery, DensityPBD, ParticleIntegrator,
+StaticBoundary, ParticleElasticBody, ElasticityModule) driving the sm_100a
+library through the C ABI, as a PhysIKA scene would: the same frames as the
+direct C-ABI calls."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import pkhot
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+LIB = os.path.join(os.path.dirname(pkhot.LIB_PATH), "libpkframework.so")
+
+
+def fw():
+    pkhot.load()
+    L = ctypes.CDLL(LIB)
+    f3 = ctypes.POINTER(ctypes.c_float)
+    L.pkf_fluid_run.argtypes = [f3, f3, ctypes.c_int, f3, f3, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, f3, f3]
+    L.pkf_elastic_run.argtypes = [f3, f3, ctypes.c_int, f3, f3, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                  ctypes.c_int, f3, f3]
+    return L
+
+
+def fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def v3(t):
+    return np.ascontiguousarray(np.asarray(t, np.float32))
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_particle_fluid_scene_equals_fused_frames(ctx):
+    sc = scenes.dam_break_small(seed=6, n_side=14)
+    x0 = sc.x.copy()
+    x0[:, 1] -= 0.0052  # the boundary acts from the first frame
+    v0 = np.random.default_rng(6).normal(0, 0.05, x0.shape).astype(np.float32)
+    n, steps = x0.shape[0], 5
+    xo, vo = np.zeros_like(x0), np.zeros_like(x0)
+    rc = fw().pkf_fluid_run(fp(x0), fp(v0), n, fp(v3(sc.lo)), fp(v3(sc.hi)), sc.spacing, sc.radius, sc.cap,
+                            sc.iterations, sc.dt, sc.sdf_spacing, 1, steps, fp(xo), fp(vo))
+    assert rc == 0
+    ctx.boundary_set_box(sc.lo, sc.hi, sc.sdf_spacing, True)
+    x, v = torch.from_numpy(x0).cuda(), torch.from_numpy(v0).cuda()
+    prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
+                           pkhot.pbd_params(sc.radius, sc.spacing, sc.rest_density, sc.iterations, sc.dt),
+                           (0.0, -9.8, 0.0))
+    for _ in range(steps):
+        ctx.pbf_step(x, v, prm)
+    ctx.check_status()
+    assert rel(xo, x.cpu().numpy()) < 1e-6
+    assert rel(vo, v.cpu().numpy()) < 1e-5
+    assert np.all(xo[:, 1] > -0.5 * sc.spacing)
+
+
+def test_particle_elastic_body_equals_module_calls(ctx):
+    sc = scenes.elastic_bar(seed=7, dims=(12, 6, 6), cap=80)
+    rng = np.random.default_rng(7)
+    x0 = (sc.x + rng.uniform(-0.02, 0.02, sc.x.shape) * sc.spacing).astype(np.float32)
+    v0 = rng.normal(0, 0.05, x0.shape).astype(np.float32)
+    n, steps = x0.shape[0], 5
+    xo, vo = np.zeros_like(x0), np.zeros_like(x0)
+    rc = fw().pkf_elastic_run(fp(x0), fp(v0), n, fp(v3(sc.lo)), fp(v3(sc.hi)), sc.horizon, sc.cap, sc.dt, steps,
+                              fp(xo), fp(vo))
+    assert rc == 0
+    x, v = torch.from_numpy(x0).cuda(), torch.from_numpy(v0).cuda()
+    idx, el, tot = ctx.nq_build(x, sc.horizon, sc.lo, sc.hi, sc.cap)
+    ctx.pd_init(x, idx, el, sc.cap, tot, sc.horizon)
+    ctx.pd_set_bulk(torch.ones(n, device="cuda"))
+    for _ in range(steps):
+        ctx.integrate(x, v, (0.0, -9.8, 0.0), sc.dt)
+        ctx.pd_solve(x, v, sc.horizon, 0.05, 0.1, 10, sc.dt)
+    ctx.check_status()
+    assert rel(xo, x.cpu().numpy()) < 1e-6
+    assert rel(vo, v.cpu().numpy()) < 1e-5
