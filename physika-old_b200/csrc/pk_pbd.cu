@@ -40,6 +40,11 @@ __device__ __forceinline__ void pair_geom(float dx, float dy, float dz, float in
     dd = fmaxf(fmaf(-(d2 * ir), inv_h, 1.0f), 0.0f);
 }
 
+#ifndef PK_PASS_BLOCK
+#define PK_PASS_BLOCK 256
+#endif
+constexpr int kPassBlock = PK_PASS_BLOCK;  // threads per block of the Jacobi passes
+
 // One quad of row entries (16 bytes, streaming: the rows are read once per
 // pass and outgrow L2).
 __device__ __forceinline__ int4 row_quad(const int4* p) { return __ldcs(p); }
@@ -48,7 +53,7 @@ __device__ __forceinline__ int4 row_quad(const int4* p) { return __ldcs(p); }
 // interleaved row.  Writes xl[s] = (x_i, lambda_i) so pass B gathers a
 // neighbour's position and lambda in one 16-byte load.  sum |grad_j|^2 is taken
 // as sum g_j^2 (|x_ij / r| = 1).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kPassBlock)
     k_pass_density(const float4* __restrict__ xs, const int* __restrict__ rows,
                    const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
                    float4* __restrict__ xl, float* __restrict__ rho_out)
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(256)
 // Pass B: x_i' = x_i + sum over U(i) of m_ij * 10 (x_i - x_j)(lambda_i +
 // lambda_j) grad(r) / r (DensityPBD.cu:158), m_ij = popcount of the two flag
 // bits; one thread per particle.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kPassBlock)
     k_pass_disp(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
                 int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
 {
@@ -172,11 +177,11 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     for (int it = 0; it < iterations; ++it) {
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
-        k_pass_density<<<nb1, 256, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+        k_pass_density<<<(unsigned)((n + kPassBlock - 1) / kPassBlock), kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
                                                     last ? c->rho : nullptr);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
-        k_pass_disp<<<nb1, 256, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+        k_pass_disp<<<(unsigned)((n + kPassBlock - 1) / kPassBlock), kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
         prof_end(c, PK_PROF_DISP, st);
         cur = c->xa;
         launches += 2;
