@@ -137,6 +137,17 @@ int pk_advect(pk_ctx* ctx, float* x, const float* v, int n, float dt, pk_stream 
 int pk_update_velocity(pk_ctx* ctx, float* v, const float* x, const float* x_old, int n,
                        float dt, pk_stream stream);
 
+/* ---------------------------------------------------- ImplicitViscosity */
+
+/* ImplicitViscosity::constrain (Dynamics/ParticleSystem/ImplicitViscosity.cu:98-128,
+ * K_ApplyViscosity :20-62): `iterations` Jacobi sweeps of
+ * v_i = v_old,i/(1+b) + (sum_j w_ij v_j / sum_j w_ij) b/(1+b) over any
+ * NeighborList<int>, b = dt*viscosity/smoothing_length, w = 45/(13 pi h^3)
+ * (1 - r/h) (VB_VisWeight :8-18).  x is read, v updated in place. */
+int pk_viscosity(pk_ctx* ctx, const float* x, float* v, int n, const int* index, const int* elements, int cap,
+                 long long total, float viscosity, float smoothing_length, int iterations, float dt,
+                 pk_stream stream);
+
 /* ---------------------------------------------------------- FixedPoints */
 
 /* FixedPoints::constrain (Dynamics/ParticleSystem/FixedPoints.cu:110-147,
@@ -183,12 +194,14 @@ typedef struct {
     int boundary;          /* 1: apply the context's box boundary first */
     float normal_friction; /* BoundaryConstraint.h:32 default 0.95 */
     float tangential_friction;
+    float viscosity;          /* > 0: ImplicitViscosity after the solve (the stock model sets 1, */
+    int viscosity_iterations; /*      PositionBasedFluidModel.cpp:69-70, 5 sweeps); 0: off */
 } pk_pbf_params;
 
 /* One dam-break frame: StaticBoundary::advance (StaticBoundary.cpp:45-59) then
- * PositionBasedFluidModel::step without viscosity
- * (Dynamics/ParticleSystem/PositionBasedFluidModel.cpp:83-101): integrator
- * begin, NeighborQuery on the current positions, integrate, DensityPBD.
+ * PositionBasedFluidModel::step (Dynamics/ParticleSystem/PositionBasedFluidModel.cpp:83-101):
+ * integrator begin, NeighborQuery on the current positions, integrate,
+ * DensityPBD, and ImplicitViscosity when p->viscosity > 0.
  * x, v (n AoS) are updated in place; rho_out may be NULL.  Asynchronous and
  * allocation-free once the context has seen `n` (capturable in a CUDA graph). */
 int pk_pbf_step(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p,

@@ -120,7 +120,10 @@ void pko_pd_solve##sfx(int n, real* x, real* v, const int* index, int cap, long 
                        const real* invK, const real* bulk, real horizon, real mu,            \
                        real lambda, int iterations, real dt);                           \
 void pko_pd_break##sfx(int n, const real* x, const int* index, int cap, long long total,     \
-                       const int* rest_idx, const real* rest_pos, unsigned char* alive, real s);
+                       const int* rest_idx, const real* rest_pos, unsigned char* alive, real s); \
+void pko_implicit_viscosity##sfx(int n, const real* x, real* v, const int* index,            \
+                                 const int* elements, int cap, long long total, real vis,    \
+                                 real h, int iterations, real dt);
 
 PKO_DECLARE(float, _f)
 PKO_DECLARE(double, _d)

@@ -53,6 +53,8 @@ def lib():
                 c_int, rp, _i32p, _i32p, c_int, c_ll, _i32p, rp]
             getattr(L, "pko_pd_inverse_k" + sfx).argtypes = [
                 c_int, _i32p, c_int, c_ll, rp, rt, rp]
+            getattr(L, "pko_implicit_viscosity" + sfx).argtypes = [
+                c_int, rp, rp, _i32p, _i32p, c_int, c_ll, rt, rt, c_int, rt]
             getattr(L, "pko_pd_break" + sfx).argtypes = [
                 c_int, rp, _i32p, c_int, c_ll, _i32p, rp, _u8p, rt]
             getattr(L, "pko_pd_solve" + sfx).argtypes = [
@@ -182,6 +184,17 @@ def pbd_constrain(x, v, index, elements, cap, h, mass, iterations, dt, dtype=np.
         n, x, v, np.ascontiguousarray(index, np.int32), np.ascontiguousarray(elements, np.int32),
         cap, _total(index, elements, cap), h, mass, iterations, dt, rho.ctypes.data)
     return x.reshape(-1, 3), v.reshape(-1, 3), rho[:n]
+
+
+def implicit_viscosity(x, v, index, elements, cap, vis, h, iterations, dt, dtype=np.float32):
+    """ImplicitViscosity::constrain on copies; returns v."""
+    sfx, dt_ = _rt(dtype)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    v = np.array(v, dt_).reshape(-1)
+    getattr(lib(), "pko_implicit_viscosity" + sfx)(
+        x.shape[0] // 3, x, v, np.ascontiguousarray(index, np.int32), np.ascontiguousarray(elements, np.int32),
+        cap, _total(index, elements, cap), vis, h, iterations, dt)
+    return v.reshape(-1, 3)
 
 
 def integrate(x, v, g, dt, f=None, dtype=np.float32):

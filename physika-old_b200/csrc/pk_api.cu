@@ -53,7 +53,7 @@ int ensure_particles(pk_ctx* c, int n)
     bool ok = regrow(c->perm, m) && regrow(c->inv, m) && regrow(c->key, m) && regrow(c->rank, m) &&
               regrow(c->count, m) && regrow(c->count_c, m) && regrow(c->offs, m + 1) &&
               regrow(c->xs_pre, m) && regrow(c->xs0, m) && regrow(c->xa, m) && regrow(c->xb, m) &&
-              regrow(c->vs, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
+              regrow(c->vs, m) && regrow(c->vv, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
               regrow(c->tau, m) && regrow(c->hcnt, m) && regrow(c->items, m + 1) &&
               regrow(c->nitems, 1);
     if (!ok) {
@@ -238,7 +238,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
     void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
-                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->rho, c->rcnt, c->tau,
+                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau,
                     c->hcnt, c->items, c->nitems,
                     c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
@@ -697,7 +697,8 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
                                p->gravity, st);
     l += pk::build_rows(c, n, g, p->nq.radius, p->nq.cap, row_cap, nullptr, nullptr, 0, st);
     l += pk::pbd_fast_solve(c, n, pk::make_spiky(p->pbd.smoothing_length), effective_mass(&p->pbd),
-                            p->pbd.iterations, p->pbd.dt, x, v, rho_out, st);
+                            p->pbd.iterations, p->pbd.dt, x, v, rho_out, st, p->viscosity,
+                            p->viscosity_iterations);
     c->launches = l;
     if ((rc = check_launch(c, what))) return rc;
     c->nq_valid = true;  // for batched scenes: the union of the scenes' lists
@@ -719,6 +720,27 @@ PK_API int pk_pbf_step_batched(pk_ctx* c, float* x, float* v, const int* scene_o
     if (nscenes < 1 || (nscenes > 1 && !scene_offsets))
         return fail(c, PK_ERR_ARG, "need at least one scene and its offsets");
     return pbf_step_impl(c, x, v, n, p, rho_out, scene_offsets, nscenes, stream, "pk_pbf_step_batched");
+}
+
+// ======================================================================
+// ImplicitViscosity
+
+PK_API int pk_viscosity(pk_ctx* c, const float* x, float* v, int n, const int* index, const int* elements, int cap,
+                        long long total, float viscosity, float smoothing_length, int iterations, float dt,
+                        pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || iterations < 0) return fail(c, PK_ERR_ARG, "negative particle or iteration count");
+    if (!(smoothing_length > 0.0f) || !(dt > 0.0f) || viscosity < 0.0f)
+        return fail(c, PK_ERR_ARG, "bad smoothing length, dt or viscosity");
+    int rc = check_list(c, n, index, elements, cap, total);
+    if (rc) return rc;
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    cudaSetDevice(c->device);
+    if ((rc = ensure_generic(c, n))) return rc;
+    c->launches = pk::viscosity_generic(c, x, v, n, index, elements, cap, total, viscosity, smoothing_length,
+                                        iterations, dt, (cudaStream_t)stream);
+    return check_launch(c, "pk_viscosity");
 }
 
 // ======================================================================

@@ -33,6 +33,7 @@ struct pk_ctx {
     float4* xa = nullptr;
     float4* xb = nullptr;     // (x, lambda) written by pass A
     float4* vs = nullptr;
+    float4* vv = nullptr;     // sorted velocities of the viscosity sweeps
     float* rho = nullptr;
     int2* rcnt = nullptr;
     uint2* tau = nullptr;

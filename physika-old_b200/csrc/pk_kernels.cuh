@@ -24,7 +24,10 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap,
 
 // pk_pbd.cu
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
-                   float* x, float* v, float* rho_out, cudaStream_t st);
+                   float* x, float* v, float* rho_out, cudaStream_t st, float viscosity = 0.f,
+                   int vis_iterations = 0);
+int viscosity_generic(pk_ctx* c, const float* x, float* v, int n, const int* index, const int* elements, int cap,
+                      long long total, float vis, float h, int iterations, float dt, cudaStream_t st);
 int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, const int* elements,
                       int cap, long long total, const Spiky& k, float mass, int iterations,
                       float dt, float* rho_out, cudaStream_t st);

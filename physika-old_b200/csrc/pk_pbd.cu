@@ -152,6 +152,93 @@ __global__ void __launch_bounds__(256)
     if (rho_out != nullptr) rho_out[i] = rho_s[s];
 }
 
+// ---- ImplicitViscosity (ImplicitViscosity.cu:8-128)
+
+// VB_VisWeight: 45/(13 pi h^3) (1 - r/h) for r <= h.
+struct ViscK {
+    float inv_h, cw, b;  // b = dt * viscosity / h
+};
+
+// DP_UpdateVelocity in sorted space: v = v_integrated + (x - x_old)/dt, kept
+// as the viscosity's v_old and first iterate.
+__global__ void __launch_bounds__(256)
+    k_vel_sorted(const float4* __restrict__ xf, const float4* __restrict__ x0, float4* __restrict__ vs,
+                 float4* __restrict__ vcur, int n, float dt)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 p = xf[s], q = x0[s], u = vs[s];
+    const float4 v = make_float4(u.x + (p.x - q.x) / dt, u.y + (p.y - q.y) / dt, u.z + (p.z - q.z) / dt, 0.f);
+    vs[s] = v;
+    vcur[s] = v;
+}
+
+// One K_ApplyViscosity sweep over N(i) (the rows' first |N(i)| entries):
+// v_i = v_old,i/(1+b) + (sum w v_j / sum w) b/(1+b); b = 0 and sum w = 1 when
+// sum w < EPSILON.
+__global__ void __launch_bounds__(256)
+    k_pass_visc(const float4* __restrict__ xs, const float4* __restrict__ vin, const float4* __restrict__ vold,
+                const int* __restrict__ rows, const int2* __restrict__ rcnt, int row_cap, int n, ViscK k_,
+                float4* __restrict__ vout)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 xi = xs[s];
+    const int na = rcnt[s].x;
+    const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
+    float tw = 0.f, dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
+    const int nq = (na + 3) >> 2;
+    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    for (int q = 0; q < nq; ++q) {
+        const int4 cur = nxt;
+        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));
+        const int ent[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (4 * q + k >= na) break;
+            const int j = ent[k] & kRowIndexMask;
+            const float4 xj = __ldg(xs + j);
+            const float4 vj = __ldg(vin + j);
+            float d2, ir, dd;
+            pair_geom(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, k_.inv_h, d2, ir, dd);
+            const float w = d2 > kEps2 ? k_.cw * dd : 0.0f;
+            tw += w;
+            dx_ = fmaf(w, vj.x, dx_);
+            dy_ = fmaf(w, vj.y, dy_);
+            dz_ = fmaf(w, vj.z, dz_);
+        }
+    }
+    const float b = tw < kEpsilon ? 0.0f : k_.b;
+    const float t = tw < kEpsilon ? 1.0f : tw;
+    const float4 vo = vold[s];
+    vout[s] = make_float4(vo.x / (1.0f + b) + dx_ / t * b / (1.0f + b), vo.y / (1.0f + b) + dy_ / t * b / (1.0f + b),
+                          vo.z / (1.0f + b) + dz_ / t * b / (1.0f + b), 0.f);
+}
+
+// Sorted -> caller order with the velocity given: x, v, outDensity.
+__global__ void __launch_bounds__(256)
+    k_finish_v(const float4* __restrict__ xf, const float4* __restrict__ vf, const float* __restrict__ rho_s,
+               const int* __restrict__ perm, int n, float* __restrict__ x, float* __restrict__ v,
+               float* __restrict__ rho_out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int i = perm[s];
+    const float4 p = xf[s], u = vf[s];
+    x[3 * i] = p.x;
+    x[3 * i + 1] = p.y;
+    x[3 * i + 2] = p.z;
+    v[3 * i] = u.x;
+    v[3 * i + 1] = u.y;
+    v[3 * i + 2] = u.z;
+    if (rho_out != nullptr) rho_out[i] = rho_s[s];
+}
+
+ViscK visc_k(float vis, float h, float dt)
+{
+    return ViscK{1.0f / h, 45.0f / (13.0f * (float)M_PI * h * h * h), dt * vis / h};
+}
+
 // Caller order -> sorted: the solver's starting state.
 __global__ void __launch_bounds__(256)
     k_gather_state(const float* __restrict__ x, const float* __restrict__ v, const int* __restrict__ perm,
@@ -165,10 +252,10 @@ __global__ void __launch_bounds__(256)
 }
 
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
-                   float* x, float* v, float* rho_out, cudaStream_t st)
+                   float* x, float* v, float* rho_out, cudaStream_t st, float viscosity, int vis_iterations)
 {
     if (n <= 0) return 0;
-    const unsigned nb1 = (unsigned)((n + 255) / 256);
+    const unsigned nb1 = (unsigned)((n + 255) / 256), nbp = (unsigned)((n + kPassBlock - 1) / kPassBlock);
     int launches = 0;
     const float4* cur = c->xs0;
     const PassK pk = pass_k(k, mass);
@@ -177,20 +264,38 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     for (int it = 0; it < iterations; ++it) {
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
-        k_pass_density<<<(unsigned)((n + kPassBlock - 1) / kPassBlock), kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
-                                                    last ? c->rho : nullptr);
+        k_pass_density<<<nbp, kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                                   last ? c->rho : nullptr);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
-        k_pass_disp<<<(unsigned)((n + kPassBlock - 1) / kPassBlock), kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+        k_pass_disp<<<nbp, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
         prof_end(c, PK_PROF_DISP, st);
         cur = c->xa;
         launches += 2;
     }
+    float* rho = (rho_out != nullptr && iterations > 0) ? rho_out : nullptr;
     prof_begin(c, PK_PROF_FINISH, st);
-    k_finish<<<nb1, 256, 0, st>>>(cur, c->xs0, c->vs, c->rho, c->perm, n, dt, x, v,
-                                  (rho_out != nullptr && iterations > 0) ? rho_out : nullptr);
+    if (viscosity > 0.f && vis_iterations > 0) {
+        // ImplicitViscosity after the solve (PositionBasedFluidModel.cpp:98), on
+        // the same rows; velocities ping-pong between vv and xb
+        k_vel_sorted<<<nb1, 256, 0, st>>>(cur, c->xs0, c->vs, c->vv, n, dt);
+        const ViscK vk = visc_k(viscosity, k.h, dt);
+        float4* vin = c->vv;
+        float4* vout = c->xb;
+        for (int t = 0; t < vis_iterations; ++t) {
+            k_pass_visc<<<nbp, kPassBlock, 0, st>>>(cur, vin, c->vs, c->rows, c->rcnt, c->row_cap, n, vk, vout);
+            float4* tmp = vin;
+            vin = vout;
+            vout = tmp;
+        }
+        k_finish_v<<<nb1, 256, 0, st>>>(cur, vin, c->rho, c->perm, n, x, v, rho);
+        launches += 2 + vis_iterations;
+    } else {
+        k_finish<<<nb1, 256, 0, st>>>(cur, c->xs0, c->vs, c->rho, c->perm, n, dt, x, v, rho);
+        ++launches;
+    }
     prof_end(c, PK_PROF_FINISH, st);
-    return launches + 1;
+    return launches;
 }
 
 int gather_state(pk_ctx* c, const float* x, const float* v, int n, cudaStream_t st)
@@ -469,6 +574,52 @@ SdfView sdf_view(const pk_ctx* c)
     s.nz = c->sdf_dims[2];
     s.inverted = c->sdf_inverted;
     return s;
+}
+
+
+// ImplicitViscosity on any NeighborList<int> in caller order (one thread per
+// particle, as K_ApplyViscosity): vout from vin (the previous iterate) and vold.
+__global__ void __launch_bounds__(256)
+    k_g_visc(const float* __restrict__ x, const float* __restrict__ vin, const float* __restrict__ vold,
+             float* __restrict__ vout, int n, const int* __restrict__ index, const int* __restrict__ elements,
+             int cap, long long total, ViscK k_)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2];
+    float tw = 0.f, d0 = 0.f, d1 = 0.f, d2v = 0.f;
+    const int m = nb_size(index, cap, total, n, i);
+    for (int e = 0; e < m; ++e) {
+        const int j = elements[nb_at(index, cap, i, e)];
+        float d2, ir, dd;
+        pair_geom(xi0 - x[3 * j], xi1 - x[3 * j + 1], xi2 - x[3 * j + 2], k_.inv_h, d2, ir, dd);
+        const float w = d2 > kEps2 ? k_.cw * dd : 0.0f;
+        tw += w;
+        d0 = fmaf(w, vin[3 * j], d0);
+        d1 = fmaf(w, vin[3 * j + 1], d1);
+        d2v = fmaf(w, vin[3 * j + 2], d2v);
+    }
+    const float b = tw < kEpsilon ? 0.0f : k_.b;
+    const float t = tw < kEpsilon ? 1.0f : tw;
+    vout[3 * i] = vold[3 * i] / (1.0f + b) + d0 / t * b / (1.0f + b);
+    vout[3 * i + 1] = vold[3 * i + 1] / (1.0f + b) + d1 / t * b / (1.0f + b);
+    vout[3 * i + 2] = vold[3 * i + 2] / (1.0f + b) + d2v / t * b / (1.0f + b);
+}
+
+int viscosity_generic(pk_ctx* c, const float* x, float* v, int n, const int* index, const int* elements, int cap,
+                      long long total, float vis, float h, int iterations, float dt, cudaStream_t st)
+{
+    if (n <= 0 || iterations <= 0) return 0;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const size_t bytes = sizeof(float) * 3 * (size_t)n;
+    const ViscK vk = visc_k(vis, h, dt);
+    // velOld and velBuf copies, then the sweep (ImplicitViscosity.cu:105-124)
+    cudaMemcpyAsync(c->g_xold, v, bytes, cudaMemcpyDeviceToDevice, st);
+    for (int t = 0; t < iterations; ++t) {
+        cudaMemcpyAsync(c->g_dpos, v, bytes, cudaMemcpyDeviceToDevice, st);
+        k_g_visc<<<nb, 256, 0, st>>>(x, c->g_dpos, c->g_xold, v, n, index, elements, cap, total, vk);
+    }
+    return iterations;
 }
 
 }  // namespace pk

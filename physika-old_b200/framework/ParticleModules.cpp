@@ -381,6 +381,29 @@ bool ElasticityModule<TDataType>::constrain()
     return true;
 }
 
+// =========================================================== ImplicitViscosity
+
+template <typename TDataType>
+ImplicitViscosity<TDataType>::ImplicitViscosity()
+{
+}
+
+template <typename TDataType>
+bool ImplicitViscosity<TDataType>::constrain()
+{
+    // ImplicitViscosity.cu:98-128
+    int num = (int)m_position.getElementCount();
+    if (num <= 0) return true;
+    auto& nbr = m_neighborhood.getValue();
+    pk_ctx* c = contextOf(this);
+    pkCheck(pk_viscosity(c, F(m_position.getValue()), F(m_velocity.getValue()), num, nbr.getIndex().getDataPtr(),
+                         nbr.getElements().getDataPtr(), nbr.getNeighborLimit(), nbr.total(),
+                         m_viscosity.getValue(), m_smoothingLength.getValue(), m_maxInteration,
+                         this->getParent()->getDt(), 0),
+            c, "ImplicitViscosity::constrain");
+    return true;
+}
+
 // ========================================================== BoundaryConstraint
 
 template <typename TDataType>
@@ -441,6 +464,16 @@ bool PositionBasedFluidModel<TDataType>::initializeImpl()
     m_velocity.connect(m_integrator->inVelocity());
     m_forceDensity.connect(m_integrator->inForceDensity());
     m_integrator->initialize();
+
+    if (m_viscosity > Real(0)) {
+        m_visModule = parent->template addConstraintModule<ImplicitViscosity<TDataType>>("viscosity");
+        m_visModule->setViscosity(m_viscosity);
+        m_smoothingLength.connect(&m_visModule->m_smoothingLength);
+        m_position.connect(&m_visModule->m_position);
+        m_velocity.connect(&m_visModule->m_velocity);
+        m_nbrQuery->outNeighborhood()->connect(&m_visModule->m_neighborhood);
+        m_visModule->initialize();
+    }
     return true;
 }
 
@@ -453,6 +486,7 @@ void PositionBasedFluidModel<TDataType>::step(float dt)
     m_nbrQuery->compute();
     m_integrator->integrate();
     m_pbdModule->constrain();
+    if (m_visModule) m_visModule->constrain();
     m_integrator->end();
 }
 
@@ -592,6 +626,7 @@ template class SummationDensity<DataType3f>;
 template class DensityPBD<DataType3f>;
 template class ParticleIntegrator<DataType3f>;
 template class ElasticityModule<DataType3f>;
+template class ImplicitViscosity<DataType3f>;
 template class BoundaryConstraint<DataType3f>;
 template class PositionBasedFluidModel<DataType3f>;
 template class ParticleSystem<DataType3f>;

@@ -152,6 +152,30 @@ private:
     Real m_breakStretch = 0;
 };
 
+// ImplicitViscosity (Dynamics/ParticleSystem/ImplicitViscosity.h:9-46): the
+// member fields and setters of the reference; constrain() is pk_viscosity.
+template <typename TDataType>
+class ImplicitViscosity : public ConstraintModule {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+    ImplicitViscosity();
+    bool constrain() override;
+    void setIterationNumber(int n) { m_maxInteration = n; }
+    void setViscosity(Real mu) { m_viscosity.setValue(mu); }
+
+    VarField<Real> m_viscosity{Real(0.05), "viscosity", "The viscosity of the fluid!", FieldType::Param, nullptr};
+    VarField<Real> m_smoothingLength{Real(0.011), "smoothing_length", "The smoothing length in SPH!",
+                                     FieldType::Param, nullptr};
+    DeviceArrayField<Coord> m_position{0, "position", "Storing the particle positions!", FieldType::In, nullptr};
+    DeviceArrayField<Coord> m_velocity{0, "velocity", "Storing the particle velocities!", FieldType::In, nullptr};
+    NeighborField<int> m_neighborhood{"neighborhood", "Storing neighboring particles' ids!", FieldType::In,
+                                      nullptr, 0, 0};
+
+private:
+    int m_maxInteration = 5;
+};
+
 // BoundaryConstraint with a box SDF (BoundaryConstraint.cu:108-117).
 template <typename TDataType>
 class BoundaryConstraint : public ConstraintModule {
@@ -172,8 +196,10 @@ private:
     bool m_inverted = true;
 };
 
-// PositionBasedFluidModel::step (PositionBasedFluidModel.cpp:83-101) without
-// the viscosity module: begin, NeighborQuery, integrate, DensityPBD, end.
+// PositionBasedFluidModel::step (PositionBasedFluidModel.cpp:83-101): begin,
+// NeighborQuery, integrate, DensityPBD, ImplicitViscosity (viscosity 1 as the
+// reference sets it, PositionBasedFluidModel.cpp:69-70; setViscosity(0) leaves
+// it out), end.
 template <typename TDataType>
 class PositionBasedFluidModel : public NumericalModel {
 public:
@@ -184,6 +210,7 @@ public:
     void setNeighborSizeLimit(int cap) { m_cap = cap; }
     void setIterationNumber(int it) { m_iterations = it; }
     void setSamplingDistance(Real d) { m_samplingDistance = d; }
+    void setViscosity(Real mu) { m_viscosity = mu; }
 
     VarField<Real> m_smoothingLength{Real(0.006)};
     DeviceArrayField<Coord> m_position{0, "position", "", FieldType::In, nullptr};
@@ -193,11 +220,13 @@ public:
     std::shared_ptr<NeighborQuery<TDataType>> m_nbrQuery;
     std::shared_ptr<DensityPBD<TDataType>> m_pbdModule;
     std::shared_ptr<ParticleIntegrator<TDataType>> m_integrator;
+    std::shared_ptr<ImplicitViscosity<TDataType>> m_visModule;
 
 protected:
     bool initializeImpl() override;
 
 private:
+    Real m_viscosity = Real(1);
     int m_cap = 0;
     int m_iterations = 3;
     Real m_samplingDistance = Real(0.005);

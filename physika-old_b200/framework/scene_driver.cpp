@@ -30,7 +30,8 @@ extern "C" {
 
 // A dam-break frame loop: SceneGraph bounds = [lo, hi], gravity (0, -9.8, 0);
 // a ParticleFluid (PositionBasedFluidModel: NeighborQuery with `cap`, radius,
-// DensityPBD with `iterations` and sampling distance `spacing`) of n particles,
+// DensityPBD with `iterations` and sampling distance `spacing`, ImplicitViscosity
+// with `viscosity` (the reference's model uses 1; 0 leaves it out)) of n particles,
 // and, when `boundary` is non-zero, a StaticBoundary cube [lo, hi] (SDF spacing
 // sdf_spacing, particles kept inside) advanced before the fluid every frame
 // (StaticBoundary.cpp:45-59).  x, v, x_out, v_out are host arrays of 3n
@@ -38,7 +39,7 @@ extern "C" {
 __attribute__((visibility("default"))) int pkf_fluid_run(const float* x, const float* v, int n, const float lo[3],
                                                          const float hi[3], float spacing, float radius, int cap,
                                                          int iterations, float dt, float sdf_spacing, int boundary,
-                                                         int steps, float* x_out, float* v_out)
+                                                         float viscosity, int steps, float* x_out, float* v_out)
 {
     try {
         SceneGraph& scene = SceneGraph::getInstance();
@@ -52,6 +53,7 @@ __attribute__((visibility("default"))) int pkf_fluid_run(const float* x, const f
         model->setNeighborSizeLimit(cap);
         model->setIterationNumber(iterations);
         model->setSamplingDistance(spacing);
+        model->setViscosity(viscosity);
         fluid->setParticles(to_coords(x, n), to_coords(v, n));
         StaticBoundary<DataType3f> walls("boundary");
         if (boundary) {

@@ -17,7 +17,7 @@ EXPORTED = [
     "pk_ctx_create", "pk_ctx_destroy", "pk_last_error", "pk_ctx_status", "pk_last_launch_count",
     "pk_ctx_profile", "pk_ctx_profile_read",
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
-    "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain",
+    "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain", "pk_viscosity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
     "pk_pbf_step_batched",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
@@ -45,7 +45,8 @@ class PbdParams(ctypes.Structure):
 class PbfParams(ctypes.Structure):
     _fields_ = [("nq", NqParams), ("pbd", PbdParams), ("gravity", ctypes.c_float * 3),
                 ("boundary", ctypes.c_int), ("normal_friction", ctypes.c_float),
-                ("tangential_friction", ctypes.c_float)]
+                ("tangential_friction", ctypes.c_float), ("viscosity", ctypes.c_float),
+                ("viscosity_iterations", ctypes.c_int)]
 
 
 class PdParams(ctypes.Structure):
@@ -82,6 +83,7 @@ def load():
         "pk_advect": ([P, P, P, I, F, P], I),
         "pk_update_velocity": ([P, P, P, P, I, F, P], I),
         "pk_fixed_points": ([P, P, P, I, P, P, P, I, P], I),
+        "pk_viscosity": ([P, P, P, I, P, P, I, LL, F, F, I, F, P], I),
         "pk_plane_constrain": ([P, P, I, ctypes.POINTER(F * 3), ctypes.POINTER(F * 3), P], I),
         "pk_boundary_set_box": ([P, ctypes.POINTER(F * 3), ctypes.POINTER(F * 3), F, I, P], I),
         "pk_boundary_constrain": ([P, P, P, I, F, F, F, P], I),
@@ -135,9 +137,9 @@ def pbd_params(smoothing_length, sampling_distance, rest_density=1000.0, iterati
 
 
 def pbf_params(nq, pbd, gravity=(0.0, -9.8, 0.0), boundary=True, normal_friction=0.95,
-               tangential_friction=0.0):
+               tangential_friction=0.0, viscosity=0.0, viscosity_iterations=5):
     return PbfParams(nq, pbd, _f3(gravity), int(bool(boundary)), float(normal_friction),
-                     float(tangential_friction))
+                     float(tangential_friction), float(viscosity), int(viscosity_iterations))
 
 
 class Context:
@@ -250,6 +252,11 @@ class Context:
     def update_velocity(self, v, x, x_old, dt):
         self._check(self.L.pk_update_velocity(self.h, _ptr(v), _ptr(x), _ptr(x_old), x.shape[0],
                                               float(dt), _stream()))
+
+    def viscosity(self, x, v, index, elements, cap, total, viscosity, smoothing_length, iterations=5, dt=1e-3):
+        self._check(self.L.pk_viscosity(self.h, _ptr(x), _ptr(v), x.shape[0], _ptr(index), _ptr(elements), cap,
+                                        total, float(viscosity), float(smoothing_length), int(iterations),
+                                        float(dt), _stream()))
 
     # ---- FixedPoints
     def fixed_points(self, x, v, ids, target, vel=None):

@@ -23,7 +23,8 @@ def fw():
     L = ctypes.CDLL(LIB)
     f3 = ctypes.POINTER(ctypes.c_float)
     L.pkf_fluid_run.argtypes = [f3, f3, ctypes.c_int, f3, f3, ctypes.c_float, ctypes.c_float, ctypes.c_int,
-                                ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, f3, f3]
+                                ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                ctypes.c_int, f3, f3]
     L.pkf_elastic_run.argtypes = [f3, f3, ctypes.c_int, f3, f3, ctypes.c_float, ctypes.c_int, ctypes.c_float,
                                   ctypes.c_int, f3, f3]
     return L
@@ -41,7 +42,10 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def test_particle_fluid_scene_equals_fused_frames(ctx):
+@pytest.mark.parametrize("vis", [1.0, 0.0])
+def test_particle_fluid_scene_equals_fused_frames(ctx, vis):
+    # vis 1: the stock PositionBasedFluidModel (ImplicitViscosity with
+    # viscosity 1); vis 0: the model without its viscosity module
     sc = scenes.dam_break_small(seed=6, n_side=14)
     x0 = sc.x.copy()
     x0[:, 1] -= 0.0052  # the boundary acts from the first frame
@@ -49,13 +53,13 @@ def test_particle_fluid_scene_equals_fused_frames(ctx):
     n, steps = x0.shape[0], 5
     xo, vo = np.zeros_like(x0), np.zeros_like(x0)
     rc = fw().pkf_fluid_run(fp(x0), fp(v0), n, fp(v3(sc.lo)), fp(v3(sc.hi)), sc.spacing, sc.radius, sc.cap,
-                            sc.iterations, sc.dt, sc.sdf_spacing, 1, steps, fp(xo), fp(vo))
+                            sc.iterations, sc.dt, sc.sdf_spacing, 1, vis, steps, fp(xo), fp(vo))
     assert rc == 0
     ctx.boundary_set_box(sc.lo, sc.hi, sc.sdf_spacing, True)
     x, v = torch.from_numpy(x0).cuda(), torch.from_numpy(v0).cuda()
     prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
                            pkhot.pbd_params(sc.radius, sc.spacing, sc.rest_density, sc.iterations, sc.dt),
-                           (0.0, -9.8, 0.0))
+                           (0.0, -9.8, 0.0), viscosity=vis)
     for _ in range(steps):
         ctx.pbf_step(x, v, prm)
     ctx.check_status()

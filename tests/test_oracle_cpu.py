@@ -115,3 +115,28 @@ def test_pd_static_lattice_stays_put(oracle):
     x1, v1 = oracle.pd_solve(sc.x, sc.v, idx, 0, el.shape[0], ridx, rpos, inv, sc.bulk, sc.horizon,
                              sc.mu, sc.lam, 10, sc.dt)
     assert np.max(np.abs(x1 - sc.x)) < 1e-5
+
+
+def test_implicit_viscosity_properties(oracle):
+    # ImplicitViscosity.cu:20-62: a uniform field is a fixed point, the sweep
+    # is linear in v, and one sweep of a two-particle pair gives the closed form
+    x = scenes.lattice(6, 6, 6, 0.005, 0.1, 3)
+    ri, re = oracle.neighbor_query(x, 0.0125, (0, 0, 0), (1, 1, 1), 0)
+    u = np.tile(np.float64([0.2, -0.1, 0.3]), (x.shape[0], 1))
+    vu = oracle.implicit_viscosity(x, u, ri, re, 0, 1.0, 0.0125, 5, 1e-3, dtype=np.float64)
+    assert np.allclose(vu, u, rtol=0, atol=1e-15)
+    rng = np.random.default_rng(3)
+    a, b = rng.normal(size=x.shape), rng.normal(size=x.shape)
+    f = lambda v: oracle.implicit_viscosity(x, v, ri, re, 0, 1.0, 0.0125, 5, 1e-3, dtype=np.float64)
+    assert np.allclose(f(2 * a - b), 2 * f(a) - f(b), rtol=0, atol=1e-12)
+    xf = oracle.implicit_viscosity(x, a, ri, re, 0, 1.0, 0.0125, 5, 1e-3)
+    assert np.abs(xf - f(a)).max() < 1e-5
+    # two particles 0.006 apart: sum w v_j / sum w = v_other; b = dt vis / h
+    x2 = np.float64([[0.5, 0.5, 0.5], [0.506, 0.5, 0.5]])
+    v2 = np.float64([[1.0, 0, 0], [-1.0, 0, 0]])
+    i2 = np.int32([0, 2])
+    e2 = np.int32([0, 1, 0, 1])  # each list holds itself (r = 0 is skipped) and the other
+    bb = 1e-3 * 1.0 / 0.0125
+    got = oracle.implicit_viscosity(x2, v2, i2, e2, 0, 1.0, 0.0125, 1, 1e-3, dtype=np.float64)
+    want = v2 / (1 + bb) + v2[::-1] * bb / (1 + bb)
+    assert np.allclose(got, want, rtol=0, atol=1e-14)
