@@ -565,6 +565,24 @@ def run_pk(args):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    # ---- the stock model's frame: the same frame plus ImplicitViscosity (viscosity 1, 5 sweeps)
+    prm_vis = pkhot.pbf_params(prm.nq, prm.pbd, sc.gravity, boundary=True, viscosity=1.0, viscosity_iterations=5)
+    vis_steps = max(3, min(args.steps, 20))
+    for _ in range(max(3, args.warmup)):
+        ctx.pbf_step(x, v, prm_vis)
+    barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(vis_steps):
+        ctx.pbf_step(x, v, prm_vis)
+    g1.record(stream)
+    barrier()
+    vis_ms = max_over_ranks(g0.elapsed_time(g1)) / vis_steps
+    ctx.check_status()
+    line["viscosity"] = {"ms_per_step": vis_ms, "value": world * n / (vis_ms / 1e3), "unit": UNIT,
+                         "stage_ms": vis_ms - ms_max / args.steps, "iterations": 5,
+                         "note": "PositionBasedFluidModel frame with ImplicitViscosity (viscosity 1) "
+                                 "on the solver rows"}
     ctx.close()
     if not args.no_batched:
         line["batched"] = measure_batched(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier,

@@ -132,6 +132,172 @@ __global__ void __launch_bounds__(kPassBlock)
     xs_out[s] = make_float4(xi.x + ax, xi.y + ay, xi.z + az, 0.f);
 }
 
+// ---- FP32x2 variants of the passes (sm_100 packed FFMA2/FADD2/FMUL2): two
+// row entries per instruction.  Each lane runs its full quads as two entry
+// pairs, then its last partial quad one entry at a time.  The sums run as two
+// interleaved partial sums (even and odd entries of each pair), so the order
+// of additions differs from the one-entry kernels; the arithmetic of each
+// pair term is identical.  d is taken as x_j - x_i (the exact negation of
+// x_i - x_j), so the accumulated gradients and displacements carry the
+// opposite sign and are negated at the end.
+
+#ifndef PK_PASS_F32X2
+#define PK_PASS_F32X2 1
+#endif
+#ifndef PK_PASS_MINB
+#define PK_PASS_MINB 1
+#endif
+
+struct Geom2 {
+    float2 dx, dy, dz, d2, ir, dd;
+};
+
+__device__ __forceinline__ void pair_geom2(const float4& a, const float4& b, const float4& xi, float inv_h, Geom2& g)
+{
+    g.dx = make_float2(a.x - xi.x, b.x - xi.x);
+    g.dy = make_float2(a.y - xi.y, b.y - xi.y);
+    g.dz = make_float2(a.z - xi.z, b.z - xi.z);
+    g.d2 = __ffma2_rn(g.dz, g.dz, __ffma2_rn(g.dy, g.dy, __fmul2_rn(g.dx, g.dx)));
+    g.ir = make_float2(rsqrtf(fmaxf(g.d2.x, 1e-30f)), rsqrtf(fmaxf(g.d2.y, 1e-30f)));
+    const float2 t = __ffma2_rn(__fmul2_rn(g.d2, g.ir), make_float2(-inv_h, -inv_h), make_float2(1.0f, 1.0f));
+    g.dd = make_float2(fmaxf(t.x, 0.0f), fmaxf(t.y, 0.0f));
+}
+
+struct DensAcc {
+    float2 rho, sg, gx, gy, gz;
+};
+
+__device__ __forceinline__ void dens_pair(const float4& a, const float4& b, const float4& xi, const PassK& k_,
+                                          DensAcc& s)
+{
+    Geom2 g;
+    pair_geom2(a, b, xi, k_.inv_h, g);
+    const float2 dd2 = __fmul2_rn(g.dd, g.dd);
+    s.rho = __ffma2_rn(make_float2(k_.cwm, k_.cwm), __fmul2_rn(dd2, g.dd), s.rho);
+    const float2 gg = __fmul2_rn(make_float2(k_.cg, k_.cg), dd2);
+    const float2 w = make_float2(g.d2.x > kEps2 ? gg.x : 0.0f, g.d2.y > kEps2 ? gg.y : 0.0f);
+    const float2 gi = __fmul2_rn(w, g.ir);
+    s.gx = __ffma2_rn(gi, g.dx, s.gx);
+    s.gy = __ffma2_rn(gi, g.dy, s.gy);
+    s.gz = __ffma2_rn(gi, g.dz, s.gz);
+    s.sg = __ffma2_rn(w, w, s.sg);
+}
+
+// One entry into the .x partial sums (the tail of a row).
+__device__ __forceinline__ void dens_one(const float4& a, const float4& xi, const PassK& k_, DensAcc& s)
+{
+    const float dx = a.x - xi.x, dy = a.y - xi.y, dz = a.z - xi.z;
+    float d2, ir, dd;
+    pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
+    const float dd2 = dd * dd;
+    s.rho.x = fmaf(k_.cwm, dd2 * dd, s.rho.x);
+    const float w = d2 > kEps2 ? k_.cg * dd2 : 0.0f;
+    const float gi = w * ir;
+    s.gx.x = fmaf(gi, dx, s.gx.x);
+    s.gy.x = fmaf(gi, dy, s.gy.x);
+    s.gz.x = fmaf(gi, dz, s.gz.x);
+    s.sg.x = fmaf(w, w, s.sg.x);
+}
+
+__global__ void __launch_bounds__(kPassBlock, PK_PASS_MINB)
+    k_pass_density2(const float4* __restrict__ xs, const int* __restrict__ rows,
+                    const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
+                    float4* __restrict__ xl, float* __restrict__ rho_out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 xi = xs[s];
+    const int na = rcnt[s].x;
+    const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
+    DensAcc a{};
+    const int nfull = na >> 2, nq = (na + 3) >> 2;
+    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    for (int q = 0; q < nfull; ++q) {
+        const int4 cur = nxt;
+        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));  // next quad in flight
+        const float4 x0 = __ldg(xs + (cur.x & kRowIndexMask)), x1 = __ldg(xs + (cur.y & kRowIndexMask));
+        const float4 x2 = __ldg(xs + (cur.z & kRowIndexMask)), x3 = __ldg(xs + (cur.w & kRowIndexMask));
+        dens_pair(x0, x1, xi, k_, a);
+        dens_pair(x2, x3, xi, k_, a);
+    }
+    const int rest = na - 4 * nfull;
+    if (rest > 0) {
+        const int ent[3] = {nxt.x, nxt.y, nxt.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k < rest) dens_one(__ldg(xs + (ent[k] & kRowIndexMask)), xi, k_, a);
+    }
+    const float rho = a.rho.x + a.rho.y, sg = a.sg.x + a.sg.y;
+    const float gx = a.gx.x + a.gx.y, gy = a.gy.x + a.gy.y, gz = a.gz.x + a.gz.y;
+    float l = sg + (gx * gx + gy * gy + gz * gz);
+    l = -(rho - 1000.0f) / (l + 0.1f);  // rest density hard-coded (DensityPBD.cu:87)
+    xl[s] = make_float4(xi.x, xi.y, xi.z, l > 0.0f ? 0.0f : l);
+    if (rho_out != nullptr) rho_out[s] = rho;
+}
+
+struct DispAcc {
+    float2 ax, ay, az;
+};
+
+__device__ __forceinline__ void disp_pair(const float4& a, const float4& b, int va, int vb, const float4& xi,
+                                          const PassK& k_, DispAcc& s)
+{
+    Geom2 g;
+    pair_geom2(a, b, xi, k_.inv_h, g);
+    const float2 mult = make_float2((float)__popc((unsigned)va >> 30), (float)__popc((unsigned)vb >> 30));
+    const float2 lw = make_float2(xi.w + a.w, xi.w + b.w);
+    const float2 c = __fmul2_rn(__fmul2_rn(__fmul2_rn(mult, lw),
+                                           __fmul2_rn(make_float2(k_.c10g, k_.c10g), __fmul2_rn(g.dd, g.dd))),
+                                g.ir);
+    const float2 cc = make_float2(g.d2.x > kEps2 ? c.x : 0.0f, g.d2.y > kEps2 ? c.y : 0.0f);
+    s.ax = __ffma2_rn(cc, g.dx, s.ax);
+    s.ay = __ffma2_rn(cc, g.dy, s.ay);
+    s.az = __ffma2_rn(cc, g.dz, s.az);
+}
+
+__device__ __forceinline__ void disp_one(const float4& a, int v, const float4& xi, const PassK& k_, DispAcc& s)
+{
+    const float mult = (float)__popc((unsigned)v >> 30);
+    const float dx = a.x - xi.x, dy = a.y - xi.y, dz = a.z - xi.z;
+    float d2, ir, dd;
+    pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
+    const float c = d2 > kEps2 ? mult * (xi.w + a.w) * (k_.c10g * (dd * dd)) * ir : 0.0f;
+    s.ax.x = fmaf(c, dx, s.ax.x);
+    s.ay.x = fmaf(c, dy, s.ay.x);
+    s.az.x = fmaf(c, dz, s.az.x);
+}
+
+__global__ void __launch_bounds__(kPassBlock, PK_PASS_MINB)
+    k_pass_disp2(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
+                 int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 xi = xl[s];
+    const int nu = rcnt[s].y;
+    const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
+    DispAcc a{};
+    const int nfull = nu >> 2, nq = (nu + 3) >> 2;
+    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    for (int q = 0; q < nfull; ++q) {
+        const int4 cur = nxt;
+        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));  // next quad in flight
+        const float4 x0 = __ldg(xl + (cur.x & kRowIndexMask)), x1 = __ldg(xl + (cur.y & kRowIndexMask));
+        const float4 x2 = __ldg(xl + (cur.z & kRowIndexMask)), x3 = __ldg(xl + (cur.w & kRowIndexMask));
+        disp_pair(x0, x1, cur.x, cur.y, xi, k_, a);
+        disp_pair(x2, x3, cur.z, cur.w, xi, k_, a);
+    }
+    const int rest = nu - 4 * nfull;
+    if (rest > 0) {
+        const int ent[3] = {nxt.x, nxt.y, nxt.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k < rest) disp_one(__ldg(xl + (ent[k] & kRowIndexMask)), ent[k], xi, k_, a);
+    }
+    // the sums hold -(displacement): d was x_j - x_i
+    xs_out[s] = make_float4(xi.x - (a.ax.x + a.ax.y), xi.y - (a.ay.x + a.ay.y), xi.z - (a.az.x + a.az.y), 0.f);
+}
+
 // Sorted -> caller order: x, v += (x - x_old)/dt (DP_UpdateVelocity,
 // DensityPBD.cu:367-378), outDensity.
 __global__ void __launch_bounds__(256)
@@ -264,11 +430,18 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     for (int it = 0; it < iterations; ++it) {
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
-        k_pass_density<<<nbp, kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
-                                                   last ? c->rho : nullptr);
+        if (PK_PASS_F32X2)
+            k_pass_density2<<<nbp, kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                                        last ? c->rho : nullptr);
+        else
+            k_pass_density<<<nbp, kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                                       last ? c->rho : nullptr);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
-        k_pass_disp<<<nbp, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+        if (PK_PASS_F32X2)
+            k_pass_disp2<<<nbp, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+        else
+            k_pass_disp<<<nbp, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
         prof_end(c, PK_PROF_DISP, st);
         cur = c->xa;
         launches += 2;
