@@ -54,12 +54,16 @@ int ensure_particles(pk_ctx* c, int n)
               regrow(c->count, m) && regrow(c->count_c, m) && regrow(c->offs, m + 1) &&
               regrow(c->xs_pre, m) && regrow(c->xs0, m) && regrow(c->xa, m) && regrow(c->xb, m) &&
               regrow(c->vs, m) && regrow(c->vv, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
-              regrow(c->tau, m) && regrow(c->hcnt, m) && regrow(c->items, m + 1) &&
+              regrow(c->tau, m) && regrow(c->tau_hint, m) && regrow(c->hcnt, m) && regrow(c->items, m + 1) &&
               regrow(c->nitems, 1);
     if (!ok) {
         c->cap_n = 0;
         return fail(c, PK_ERR_NOMEM, "device allocation of particle scratch failed");
     }
+    // no pivot yet: all ones sits above every distance, so the first selection
+    // takes the plain rounds
+    if (cudaMemset(c->tau_hint, 0xff, sizeof(unsigned) * m) != cudaSuccess)
+        return fail(c, PK_ERR_CUDA, "cudaMemset of the selection pivots failed");
     c->cap_n = n;
     return PK_OK;
 }
@@ -238,7 +242,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
     void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
-                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau,
+                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau, c->tau_hint,
                     c->hcnt, c->items, c->nitems,
                     c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,

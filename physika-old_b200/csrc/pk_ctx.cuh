@@ -37,6 +37,7 @@ struct pk_ctx {
     float* rho = nullptr;
     int2* rcnt = nullptr;
     uint2* tau = nullptr;
+    unsigned* tau_hint = nullptr;  // caller order: d2 bits of the last frame's tau (selection pivot)
 
     // ---- rows (capacity cap_rows entries)
     long long cap_rows = 0;

@@ -337,11 +337,9 @@ struct MemSrc {
     }
 };
 
-// Few keys above tau (E = c - cap small): tau is the (E+1)-th largest key.
-// Keys (d2 bits, index) pack into 64-bit integers whose order is the key
-// order; each lane sorts its <= 4 keys descending, then E+1 rounds take the
-// warp's largest head (two 32-bit warp maxima: d2, then index among equal d2)
-// and the owning lane advances.
+// Few keys above tau (E = c - cap small, rows of at most 128 hits): tau is
+// found by rounds of warp maxima over 64-bit keys (d2 bits, index), whose
+// integer order is the key order.
 constexpr int kTopMax = 32;
 
 __device__ __forceinline__ void cswap_desc(unsigned long long& a, unsigned long long& b)
@@ -351,30 +349,68 @@ __device__ __forceinline__ void cswap_desc(unsigned long long& a, unsigned long 
     b = lo;
 }
 
-// h: this lane's entries lane, lane+32, lane+64, lane+96 of the row (0 past c).
-__device__ __forceinline__ uint2 select_top(const uint2 (&h)[4], int E)
+// The (R)-th largest of the warp's keys (R >= 1): each lane sorts its <= 4
+// keys descending, then R rounds take the warp's largest head (two 32-bit
+// warp maxima: high word, then low word among equal high words) and the owning
+// lane advances.  Returns the last key taken as (high, low).
+__device__ __forceinline__ uint2 take_largest(unsigned long long (&k)[4], int R)
 {
-    unsigned long long k[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) k[q] = ((unsigned long long)h[q].y << 32) | h[q].x;
     cswap_desc(k[0], k[1]);
     cswap_desc(k[2], k[3]);
     cswap_desc(k[0], k[2]);
     cswap_desc(k[1], k[3]);
     cswap_desc(k[1], k[2]);
-    unsigned md = 0u, mt = 0u;
-    for (int r = 0; r <= E; ++r) {
-        const unsigned hd = (unsigned)(k[0] >> 32), ht = (unsigned)k[0];
-        md = __reduce_max_sync(kFull, hd);
-        mt = __reduce_max_sync(kFull, hd == md ? ht : 0u);
-        if (hd == md && ht == mt) {
+    unsigned mh = 0u, ml = 0u;
+    for (int r = 0; r < R; ++r) {
+        const unsigned hh = (unsigned)(k[0] >> 32), hl = (unsigned)k[0];
+        mh = __reduce_max_sync(kFull, hh);
+        ml = __reduce_max_sync(kFull, hh == mh ? hl : 0u);
+        if (hh == mh && hl == ml) {
             k[0] = k[1];
             k[1] = k[2];
             k[2] = k[3];
             k[3] = 0ull;
         }
     }
-    return make_uint2(md, mt);
+    return make_uint2(mh, ml);
+}
+
+// tau from a pivot: the previous frame's tau distance of the same particle
+// (d2 bits `hint`).  With L keys at or below the pivot, tau is the
+// (L - cap + 1)-th largest of those when L >= cap, else the (cap - L)-th
+// smallest of the keys above it (taken as the largest of the complemented
+// keys).  Positions move little between frames, so |L - cap| is small and
+// few rounds run; the result is the same key whatever the pivot.  A pivot
+// that saves nothing falls back to the E + 1 rounds of select_top.
+// h: entries lane, lane+32, lane+64, lane+96 of the row (c <= 128).
+__device__ __forceinline__ uint2 select_pivot(const uint2 (&h)[4], int c, int cap, unsigned hint, int lane)
+{
+    const unsigned long long P = ((unsigned long long)hint << 32) | 0xffffffffull;
+    unsigned long long k[4];
+    bool ok[4];
+    int le = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        ok[q] = q * 32 + lane < c;
+        k[q] = ((unsigned long long)h[q].y << 32) | h[q].x;
+        le += (ok[q] && k[q] <= P) ? 1 : 0;
+    }
+    le = (int)__reduce_add_sync(kFull, (unsigned)le);
+    const int E = c - cap;
+    if (le >= cap && le - cap + 1 <= E) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) k[q] = (ok[q] && k[q] <= P) ? k[q] : 0ull;
+        return take_largest(k, le - cap + 1);
+    }
+    if (le < cap && cap - le <= E) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) k[q] = (ok[q] && k[q] > P) ? ~k[q] : 0ull;
+        const uint2 r = take_largest(k, cap - le);
+        return make_uint2(~r.x, ~r.y);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) k[q] = ok[q] ? k[q] : 0ull;
+    return take_largest(k, E + 1);
 }
 
 // A warp takes 32 consecutive particles: lane l reads the count of particle
@@ -383,7 +419,7 @@ __device__ __forceinline__ uint2 select_top(const uint2 (&h)[4], int E)
 // and lane l writes tau of particle base + l.
 __global__ void __launch_bounds__(kSelWarps * 32, 1)
     k_select(const uint2* __restrict__ hits, const int* __restrict__ hcnt, int n, int cap, int row_cap,
-             float T, uint2* __restrict__ tau)
+             float T, uint2* __restrict__ tau, const int* __restrict__ perm, unsigned* __restrict__ tau_hint)
 {
     __shared__ SelSmem sm[kSelWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -395,6 +431,8 @@ __global__ void __launch_bounds__(kSelWarps * 32, 1)
         const int c_l = s_l < n ? __ldg(hcnt + s_l) : 0;
         uint2 tau_l = make_uint2(0x7f800000u, 0x7fffffffu);  // every hit is in N(i)
         unsigned need = __ballot_sync(kFull, c_l > cap);
+        const int id_l = c_l > cap ? __ldg(perm + s_l) : 0;
+        const unsigned hint_l = c_l > cap ? tau_hint[id_l] : 0xffffffffu;
         // rows of at most 128 hits are read into registers one particle ahead,
         // so the next row's loads overlap the current selection
         uint2 hn[4];
@@ -420,7 +458,7 @@ __global__ void __launch_bounds__(kSelWarps * 32, 1)
             prefetch(need, hn);
             uint2 r;
             if (c <= 32 * kSelRegChunks && c - cap + 1 <= kTopMax) {
-                r = select_top(h, c - cap);
+                r = select_pivot(h, c, cap, __shfl_sync(kFull, hint_l, q), lane);
             } else if (c <= 32 * kSelRegChunks) {
                 RegSrc src;
 #pragma unroll
@@ -435,6 +473,7 @@ __global__ void __launch_bounds__(kSelWarps * 32, 1)
             if (lane == q) tau_l = r;
         }
         if (s_l < n) tau[s_l] = tau_l;
+        if (c_l > cap) tau_hint[id_l] = tau_l.x;  // the next frame's pivot
     }
 }
 
@@ -568,7 +607,8 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     ++launches;
     if (capped) {
         const int sb = (int)std::min<long long>(((long long)n + 32 * kSelWarps - 1) / (32 * kSelWarps), (long long)sms * 8);
-        k_select<<<sb, kSelWarps * 32, 0, st>>>(c->hits, c->hcnt, n, cap, row_cap, A.T, c->tau);
+        k_select<<<sb, kSelWarps * 32, 0, st>>>(c->hits, c->hcnt, n, cap, row_cap, A.T, c->tau, c->perm,
+                                                c->tau_hint);
         ++launches;
     }
     if (dyn_pub) {

@@ -54,6 +54,22 @@ def test_dam_break_2m_shape_small_block(oracle, cap):
     assert_same_lists(oracle, sc.x, sc.radius, sc.lo, sc.hi, cap)
 
 
+@pytest.mark.parametrize("cap", [60, 20])
+def test_repeated_builds_with_moving_particles(oracle, cap):
+    # the capped selection starts from each particle's previous tau: lists of
+    # later frames on the same context (small moves, a large jump, a shuffled
+    # caller order so the carried-over pivots belong to other particles) must
+    # stay bit-exact
+    sc = scenes.dam_break_small(seed=9, n_side=20)
+    rng = np.random.default_rng(9)
+    x = sc.x.copy()
+    for step, amp in enumerate((0.0, 0.02, 0.05, 0.5, 0.01)):
+        x = (x + rng.uniform(-amp, amp, x.shape) * sc.spacing).astype(np.float32)
+        if step == 3:
+            x = x[rng.permutation(x.shape[0])]
+        assert_same_lists(oracle, x, sc.radius, sc.lo, sc.hi, cap)
+
+
 def test_empty_and_single(ctx, oracle):
     for n in (0, 1):
         x = np.full((n, 3), 0.5, np.float32)
