@@ -13,17 +13,19 @@
 //     lane holds the pass's particles in registers and takes one candidate of
 //     each 32-wide chunk of the 27 neighbour ranges (a coalesced load), so a
 //     lane runs 16 independent pair tests per chunk; one ballot per particle
-//     appends the chunk's hits to its row in candidate order.  The hit test
-//     compares the rounded squared distance with the precomputed float T
-//     (sqrt_rn(d2) < h  <=>  d2 < T, sqrt_rn being monotone), so no square
-//     root is taken.  The same sweep counts the hits below a narrow window
-//     around the particle's previous tau and collects the hits inside it;
-//     when the cap-th smallest key falls in the window it is ranked there
-//     exactly: tau_i.  Otherwise further sweeps refine a 32-bin histogram of
-//     d2 until the bin holding the cap-th key fits the slots.  Keys are
-//     (d2, sorted index): sqrt_rn is monotone, so this order agrees with the
-//     reference's distance order except among hits at exactly equal
-//     distance, which the reference orders by arrival.
+//     appends the chunk's hits (sorted index, d2) to its hit row in candidate
+//     order.  The hit test compares the rounded squared distance with the
+//     precomputed float T (sqrt_rn(d2) < h  <=>  d2 < T, sqrt_rn being
+//     monotone), so no square root is taken.
+//   k_select (capped lists, a warp per over-cap row): tau_i, the cap-th
+//     smallest key (d2, sorted index) of the row.  Rows of at most 128 hits
+//     are held in registers and tau is taken by rounds of warp maxima over
+//     64-bit keys, pivoted on the particle's tau of the previous frame so only
+//     |#keys below the pivot - cap| + 1 rounds run; longer rows narrow a
+//     32-bin histogram of d2 until the bin holding the cap-th key fits a warp.
+//     sqrt_rn is monotone, so the key order agrees with the reference's
+//     distance order except among hits at exactly equal distance, which the
+//     reference orders by arrival.
 //   k_emit (8 lanes per particle): re-reads the hit row, marks a = key <= tau_i
 //     (j in N(i)) and b = key' <= tau_j (i in N(j)), compacts in place with
 //     a-entries first, then b-only entries, and writes the public NeighborList
@@ -417,7 +419,10 @@ __device__ __forceinline__ uint2 select_pivot(const uint2 (&h)[4], int c, int ca
 // base + l, the particles with more than cap hits are selected one after the
 // other (their rows loaded into registers when they hold at most 128 hits),
 // and lane l writes tau of particle base + l.
-__global__ void __launch_bounds__(kSelWarps * 32, 1)
+#ifndef PK_SEL_MIN_BLOCKS
+#define PK_SEL_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
     k_select(const uint2* __restrict__ hits, const int* __restrict__ hcnt, int n, int cap, int row_cap,
              float T, uint2* __restrict__ tau, const int* __restrict__ perm, unsigned* __restrict__ tau_hint)
 {
