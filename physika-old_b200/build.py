@@ -42,7 +42,7 @@ def build_framework(force=False, verbose=True):
     libpkhot.so (found next to it at run time)."""
     out = os.path.join(HERE, "lib", "libpkframework.so")
     fw = os.path.join(HERE, "framework")
-    srcs = [os.path.join(fw, s) for s in ("ParticleModules.cpp", "scene_driver.cpp")]
+    srcs = [os.path.join(fw, s) for s in ("ParticleModules.cpp", "ParticleIO.cpp", "scene_driver.cpp")]
     deps = srcs + glob.glob(os.path.join(fw, "*.h")) + [os.path.join(ROOT, "include", "pk_hot.h")]
     if not force and not _newer(out, deps):
         return out

@@ -236,10 +236,16 @@ private:
 template <typename TDataType>
 class ParticleSystem : public Node {
 public:
+    typedef typename TDataType::Real Real;
     typedef typename TDataType::Coord Coord;
     explicit ParticleSystem(std::string name = "default") : Node(std::move(name)) {}
     void setParticles(const std::vector<Coord>& pos, const std::vector<Coord>& vel);
     void getParticles(std::vector<Coord>& pos, std::vector<Coord>& vel);
+    // ParticleSystem::loadParticles (ParticleSystem.cpp:34-97), in ParticleIO.cpp:
+    // an OBJ file's vertices, a ball or a box lattice, at rest.
+    void loadParticles(std::string filename);
+    void loadParticles(Coord center, Real r, Real distance);
+    void loadParticles(Coord lo, Coord hi, Real distance);
 
     DEF_EMPTY_CURRENT_ARRAY(Position, Coord, DeviceType::GPU, "Particle position");
     DEF_EMPTY_CURRENT_ARRAY(Velocity, Coord, DeviceType::GPU, "Particle velocity");

@@ -8,6 +8,7 @@
 #include <memory>
 #include <vector>
 
+#include "ParticleIO.h"
 #include "ParticleModules.h"
 
 using namespace PhysIKA;
@@ -73,6 +74,56 @@ __attribute__((visibility("default"))) int pkf_fluid_run(const float* x, const f
     } catch (const std::exception& e) {
         std::fprintf(stderr, "pkf_fluid_run: %s\n", e.what());
         return 2;
+    }
+}
+
+// The dam-break loop of pkf_fluid_run on particles loaded from an OBJ file
+// (ParticleSystem::loadParticles(filename)), at rest, with a ParticleWriter
+// attached to the fluid's positions: after every `write_every`-th frame it
+// writes <out_path><prefix><index>.txt (color mapping 0).  Returns the number
+// of particles, or a negative value after printing the error.
+__attribute__((visibility("default"))) int pkf_fluid_obj_run(const char* obj_path, const float lo[3],
+                                                             const float hi[3], float spacing, float radius,
+                                                             int cap, int iterations, float dt, float sdf_spacing,
+                                                             int boundary, float viscosity, int steps,
+                                                             const char* out_path, const char* prefix,
+                                                             int write_every)
+{
+    try {
+        SceneGraph& scene = SceneGraph::getInstance();
+        scene.setLowerBound(Vector3f(lo[0], lo[1], lo[2]));
+        scene.setUpperBound(Vector3f(hi[0], hi[1], hi[2]));
+        scene.setGravity(Vector3f(0.0f, -9.8f, 0.0f));
+        auto fluid = std::make_shared<ParticleFluid<DataType3f>>("fluid");
+        fluid->setDt(dt);
+        auto model = fluid->getModel();
+        model->m_smoothingLength.setValue(radius);
+        model->setNeighborSizeLimit(cap);
+        model->setIterationNumber(iterations);
+        model->setSamplingDistance(spacing);
+        model->setViscosity(viscosity);
+        fluid->loadParticles(std::string(obj_path));
+        const int n = (int)fluid->currentPosition()->getElementCount();
+        StaticBoundary<DataType3f> walls("boundary");
+        if (boundary) {
+            walls.loadCube(Vector3f(lo[0], lo[1], lo[2]), Vector3f(hi[0], hi[1], hi[2]), sdf_spacing, true);
+            walls.addParticleSystem(fluid);
+        }
+        ParticleWriter<DataType3f> writer;
+        writer.setOutputPath(out_path ? out_path : "");
+        writer.setNamePrefix(prefix ? prefix : "test_");
+        fluid->currentPosition()->connect(&writer.m_position);
+        writer.m_color_mapping.setElementCount(n);
+        if (!fluid->initialize()) return -1;
+        for (int s = 0; s < steps; ++s) {
+            if (boundary) walls.advance(dt);
+            fluid->advance(dt);
+            if (write_every > 0 && (s + 1) % write_every == 0 && !writer.execute()) return -3;
+        }
+        return n;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "pkf_fluid_obj_run: %s\n", e.what());
+        return -2;
     }
 }
 

@@ -88,3 +88,34 @@ def test_particle_elastic_body_equals_module_calls(ctx):
     ctx.check_status()
     assert rel(xo, x.cpu().numpy()) < 1e-6
     assert rel(vo, v.cpu().numpy()) < 1e-5
+
+
+def test_particle_fluid_from_obj_with_writer(ctx, tmp_path):
+    # ParticleSystem::loadParticles(filename) + ParticleWriter frames: the
+    # written frames equal the frames of the same scene started from the
+    # same (parsed) positions
+    sc = scenes.dam_break_small(seed=8, n_side=12)
+    x0 = sc.x.copy()
+    obj = tmp_path / "block.obj"
+    obj.write_text("".join(f"v {a:.9g} {b:.9g} {c:.9g}\n" for a, b, c in x0))
+    L = fw()
+    f3 = ctypes.POINTER(ctypes.c_float)
+    L.pkf_fluid_obj_run.argtypes = [ctypes.c_char_p, f3, f3, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                    ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+    L.pkf_read_frame.argtypes = [ctypes.c_char_p, f3, f3, ctypes.c_int]
+    out = str(tmp_path) + os.sep
+    n = L.pkf_fluid_obj_run(str(obj).encode(), fp(v3(sc.lo)), fp(v3(sc.hi)), sc.spacing, sc.radius, sc.cap,
+                            sc.iterations, sc.dt, sc.sdf_spacing, 1, 1.0, 4, out.encode(), b"frame_", 2)
+    assert n == x0.shape[0]
+    n_steps = {0: 2, 1: 4}
+    for k, steps in n_steps.items():
+        xf, cf = np.zeros_like(x0), np.ones(n, np.float32)
+        assert L.pkf_read_frame(f"{out}frame_{k}.txt".encode(), fp(xf), fp(cf), n) == n
+        assert np.all(cf == 0)
+        xo, vo = np.zeros_like(x0), np.zeros_like(x0)
+        v0 = np.zeros_like(x0)
+        assert L.pkf_fluid_run(fp(x0), fp(v0), n, fp(v3(sc.lo)), fp(v3(sc.hi)), sc.spacing, sc.radius, sc.cap,
+                               sc.iterations, sc.dt, sc.sdf_spacing, 1, 1.0, steps, fp(xo), fp(vo)) == 0
+        assert np.array_equal(xf, xo), k
+    assert not os.path.exists(f"{out}frame_2.txt")
