@@ -268,6 +268,68 @@ int pk_pd_set_bulk(pk_ctx* ctx, const float* bulk, int n, pk_stream stream);
 int pk_pd_solve(pk_ctx* ctx, float* x, float* v, int n, const pk_pd_params* p,
                 pk_stream stream);
 
+/* The steps of ElasticityModule::solveElasticity (ElasticityModule.cu:404-421)
+ * one at a time, for solvers that interleave other constraints between the
+ * projection iterations (ElastoplasticityModule::solveElasticity,
+ * Dynamics/ParticleSystem/ElastoplasticityModule.cu:240-262, runs a one-
+ * iteration DensityPBD after each):
+ *   pk_pd_compute_inverse_k: K^-1 of the current rest shape (computeInverseK,
+ *     ElasticityModule.cu:390-400; plasticity moves the rest shape);
+ *   pk_pd_begin: m_position_old = x and the bond weights of the current bulk
+ *     stiffness;
+ *   pk_pd_enforce: one EM_EnforceElasticity + K_UpdatePosition against that
+ *     x_old (x in place);
+ *   pk_pd_update_velocity: v += (x - x_old)/dt (K_UpdateVelocity :295-306).
+ * p->iterations is not used by these; p->break_stretch must be 0. */
+int pk_pd_compute_inverse_k(pk_ctx* ctx, float horizon, pk_stream stream);
+int pk_pd_begin(pk_ctx* ctx, const float* x, int n, const pk_pd_params* p, pk_stream stream);
+int pk_pd_enforce(pk_ctx* ctx, float* x, int n, const pk_pd_params* p, pk_stream stream);
+int pk_pd_update_velocity(pk_ctx* ctx, const float* x, float* v, int n, float dt, pk_stream stream);
+
+/* ------------------------------------ ElastoplasticityModule / FractureModule */
+
+typedef struct {
+    float horizon; /* inHorizon */
+    float mu;      /* ElasticityModule m_mu */
+    float lambda;  /* ElasticityModule m_lambda */
+    float A;       /* computeA(): 6 c cos(phi) / (3 + sin(phi)) / sqrt(3) (ElastoplasticityModule.h:53-58) */
+    float B;       /* computeB(): 2 sin(phi) / (3 + sin(phi)) / sqrt(3) (:61-65) */
+} pk_plastic_params;
+
+/* ElastoplasticityModule::rotateRestShape (EM_RotateRestShape,
+ * ElastoplasticityModule.cu:568-657): each particle's rest bonds rotated by
+ * the polar rotation of its deformation gradient (SmoothKernel weights over
+ * the rest shape). */
+int pk_pd_rotate_rest_shape(pk_ctx* ctx, const float* x, int n, float horizon, pk_stream stream);
+
+/* ElastoplasticityModule::applyYielding (:273-307): PM_ComputeInvariants
+ * (:43-163, Drucker-Prager on I1 and J2 with the context's bulk stiffness)
+ * then PM_ApplyYielding (:165-226, rest bonds moved by the mean yield of
+ * their two ends). */
+int pk_pd_apply_yielding(pk_ctx* ctx, const float* x, int n, const pk_plastic_params* p, pk_stream stream);
+
+/* ElastoplasticityModule::reconstructRestShape (:483-531): particles flagged
+ * as yielding (all of them when reconstruct_all, enableFullyReconstruction)
+ * take their current neighbours (index/elements/cap/total: a NeighborList of
+ * the current positions) as rest bonds placed by the inverse deformation
+ * (PM_ComputeInverseDeformation :389-471, PM_ReconstructRestShape :309-371);
+ * the others keep theirs.  The rest shape becomes a CSR list.  Synchronises
+ * the stream (the new bond count sizes the list). */
+int pk_pd_reconstruct_rest_shape(pk_ctx* ctx, const float* x, int n, const int* index, const int* elements,
+                                 int cap, long long total, float horizon, int reconstruct_all,
+                                 pk_stream stream);
+
+/* FractureModule::applyPlasticity (Dynamics/ParticleSystem/FractureModule.cu:107-128):
+ * particles past the Drucker-Prager limit lose their bulk stiffness. */
+int pk_pd_fracture(pk_ctx* ctx, const float* x, int n, const pk_plastic_params* p, pk_stream stream);
+
+/* State readers: the yield fields of the last pk_pd_apply_yielding (n floats
+ * each, any may be NULL), the bulk stiffness, and the rest-shape layout
+ * (index: n counts (cap > 0) or CSR offsets (cap == 0); any may be NULL). */
+int pk_pd_get_yield(pk_ctx* ctx, float* yield_i1, float* yield_j2, float* i1, pk_stream stream);
+int pk_pd_get_bulk(pk_ctx* ctx, float* bulk, pk_stream stream);
+int pk_pd_rest_layout(pk_ctx* ctx, int* index, int* cap, long long* total, pk_stream stream);
+
 /* Copies the frozen rest shape out: rest_idx/rest_pos in the NeighborList
  * layout the rest shape was built with (TPair index/pos, Dynamics/ParticleSystem/NeighborData.h:6-21). */
 int pk_pd_get_rest_shape(pk_ctx* ctx, int* rest_idx, float* rest_pos, float* inv_k,

@@ -476,6 +476,7 @@ void pko_sdf_constrain(int n, float* x, float* v, const pko_sdf* s, const float*
 #define RSQRT sqrtf
 #define FMA fmaf
 #include "pk_oracle_solver.inc"
+#include "pk_oracle_plastic.inc"
 #undef real
 #undef SFX
 #undef RSQRT
@@ -527,6 +528,7 @@ void pko_kernels_f(int n, const float* r, float h, float* out5)
 #define RSQRT sqrt
 #define FMA fma
 #include "pk_oracle_solver.inc"
+#include "pk_oracle_plastic.inc"
 #undef real
 #undef SFX
 #undef RSQRT

@@ -123,7 +123,35 @@ void pko_pd_break##sfx(int n, const real* x, const int* index, int cap, long lon
                        const int* rest_idx, const real* rest_pos, unsigned char* alive, real s); \
 void pko_implicit_viscosity##sfx(int n, const real* x, real* v, const int* index,            \
                                  const int* elements, int cap, long long total, real vis,    \
-                                 real h, int iterations, real dt);
+                                 real h, int iterations, real dt);                           \
+void pko_pd_enforce##sfx(int n, real* x, const real* xold, const int* index, int cap,        \
+                         long long total, const int* rest_idx, const real* rest_pos,         \
+                         const real* invK, const real* bulk, real horizon, real mu,          \
+                         real lambda);                                                       \
+void pko_pd_rotate_rest_shape##sfx(int n, const real* x, const int* index, int cap,          \
+                                   long long total, const int* rest_idx, real* rest_pos,     \
+                                   real h);                                                  \
+void pko_pd_invariants##sfx(int n, const real* x, const int* index, int cap, long long total,\
+                            const int* rest_idx, const real* rest_pos, const real* bulk,     \
+                            real h, real A, real B, real mu, real lambda, real* yield_i1,    \
+                            real* yield_j2, real* i1, unsigned char* byield);                \
+void pko_pd_apply_yielding##sfx(int n, const real* x, const int* index, int cap,             \
+                                long long total, const int* rest_idx, real* rest_pos,        \
+                                const real* yield_i1, const real* yield_j2, const real* i1); \
+void pko_pd_inverse_deformation##sfx(int n, const real* x, const int* index, int cap,        \
+                                     long long total, const int* rest_idx,                   \
+                                     const real* rest_pos, real h, real* invF);              \
+void pko_pd_recon_sizes##sfx(int n, const unsigned char* byield, const int* nbr_index,       \
+                             int nbr_cap, long long nbr_total, const int* index, int cap,    \
+                             long long total, int* sizes);                                   \
+void pko_pd_recon_fill##sfx(int n, const real* x, unsigned char* byield, const real* invF,   \
+                            const int* nbr_index, const int* nbr_elements, int nbr_cap,      \
+                            long long nbr_total, const int* index, int cap, long long total, \
+                            const int* rest_idx, const real* rest_pos, const int* off,       \
+                            int* new_idx, real* new_pos);                                    \
+void pko_pd_fracture##sfx(int n, const real* x, const int* index, int cap, long long total,  \
+                          const int* rest_idx, const real* rest_pos, real* bulk, real h,     \
+                          real A, real B, real mu, real lambda);
 
 PKO_DECLARE(float, _f)
 PKO_DECLARE(double, _d)

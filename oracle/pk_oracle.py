@@ -60,6 +60,23 @@ def lib():
             getattr(L, "pko_pd_solve" + sfx).argtypes = [
                 c_int, rp, rp, _i32p, c_int, c_ll, _i32p, rp, ctypes.c_void_p, rp, rp,
                 rt, rt, rt, c_int, rt]
+            getattr(L, "pko_pd_enforce" + sfx).argtypes = [
+                c_int, rp, rp, _i32p, c_int, c_ll, _i32p, rp, rp, rp, rt, rt, rt]
+            getattr(L, "pko_pd_rotate_rest_shape" + sfx).argtypes = [
+                c_int, rp, _i32p, c_int, c_ll, _i32p, rp, rt]
+            getattr(L, "pko_pd_invariants" + sfx).argtypes = [
+                c_int, rp, _i32p, c_int, c_ll, _i32p, rp, rp, rt, rt, rt, rt, rt, rp, rp, rp, _u8p]
+            getattr(L, "pko_pd_apply_yielding" + sfx).argtypes = [
+                c_int, rp, _i32p, c_int, c_ll, _i32p, rp, rp, rp, rp]
+            getattr(L, "pko_pd_inverse_deformation" + sfx).argtypes = [
+                c_int, rp, _i32p, c_int, c_ll, _i32p, rp, rt, rp]
+            getattr(L, "pko_pd_recon_sizes" + sfx).argtypes = [
+                c_int, _u8p, _i32p, c_int, c_ll, _i32p, c_int, c_ll, _i32p]
+            getattr(L, "pko_pd_recon_fill" + sfx).argtypes = [
+                c_int, rp, _u8p, rp, _i32p, _i32p, c_int, c_ll, _i32p, c_int, c_ll, _i32p, rp, _i32p,
+                _i32p, rp]
+            getattr(L, "pko_pd_fracture" + sfx).argtypes = [
+                c_int, rp, _i32p, c_int, c_ll, _i32p, rp, rp, rt, rt, rt, rt, rt]
         _LIB = L
     return _LIB
 
@@ -284,3 +301,123 @@ def pd_solve(x, v, index, cap, total, rest_idx, rest_pos, invK, bulk, horizon, m
         np.ascontiguousarray(invK, dt_).reshape(-1), np.ascontiguousarray(bulk, dt_),
         horizon, mu, lam, iterations, dt)
     return x.reshape(-1, 3), v.reshape(-1, 3)
+
+
+# ---- ElastoplasticityModule / FractureModule (pk_oracle_plastic.inc)
+
+class RestShape:
+    """A peridynamics rest shape in the NeighborList<TPair> layouts: fixed
+    (cap > 0, index = counts) or CSR (cap == 0, index = offsets)."""
+
+    def __init__(self, index, cap, total, idx, pos):
+        self.index = np.ascontiguousarray(index, np.int32)
+        self.cap, self.total = int(cap), int(total)
+        self.idx = np.ascontiguousarray(idx, np.int32)
+        self.pos = np.ascontiguousarray(pos).reshape(-1)
+
+    def args(self, dt_):
+        self.pos = np.ascontiguousarray(self.pos, dt_)
+        return self.index, self.cap, self.total, self.idx, self.pos
+
+    def copy(self):
+        return RestShape(self.index.copy(), self.cap, self.total, self.idx.copy(), self.pos.copy())
+
+
+def pd_enforce(x, xold, rs, invK, bulk, horizon, mu, lam, dtype=np.float32):
+    """One EM_EnforceElasticity + K_UpdatePosition against x_old; returns x."""
+    sfx, dt_ = _rt(dtype)
+    x = np.array(x, dt_).reshape(-1)
+    index, cap, total, idx, pos = rs.args(dt_)
+    getattr(lib(), "pko_pd_enforce" + sfx)(
+        x.shape[0] // 3, x, np.ascontiguousarray(xold, dt_).reshape(-1), index, cap, total, idx, pos,
+        np.ascontiguousarray(invK, dt_).reshape(-1), np.ascontiguousarray(bulk, dt_), horizon, mu, lam)
+    return x.reshape(-1, 3)
+
+
+def pd_rotate_rest_shape(x, rs, h, dtype=np.float32):
+    """EM_RotateRestShape on a copy of the rest shape; returns the new RestShape."""
+    sfx, dt_ = _rt(dtype)
+    out = rs.copy()
+    index, cap, total, idx, pos = out.args(dt_)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    getattr(lib(), "pko_pd_rotate_rest_shape" + sfx)(x.shape[0] // 3, x, index, cap, total, idx, pos, h)
+    return out
+
+
+def pd_invariants(x, rs, bulk, h, A, B, mu, lam, byield, dtype=np.float32):
+    """PM_ComputeInvariants: (yield_I1, yield_J2, I1, byield)."""
+    sfx, dt_ = _rt(dtype)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    n = x.shape[0] // 3
+    index, cap, total, idx, pos = rs.args(dt_)
+    y1, y2, i1 = np.zeros(max(n, 1), dt_), np.zeros(max(n, 1), dt_), np.zeros(max(n, 1), dt_)
+    by = np.array(byield, np.uint8)
+    getattr(lib(), "pko_pd_invariants" + sfx)(n, x, index, cap, total, idx, pos, np.ascontiguousarray(bulk, dt_),
+                                               h, A, B, mu, lam, y1, y2, i1, by)
+    return y1[:n], y2[:n], i1[:n], by
+
+
+def pd_apply_yielding(x, rs, y1, y2, i1, dtype=np.float32):
+    """PM_ApplyYielding on a copy of the rest shape; returns the new RestShape."""
+    sfx, dt_ = _rt(dtype)
+    out = rs.copy()
+    index, cap, total, idx, pos = out.args(dt_)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    getattr(lib(), "pko_pd_apply_yielding" + sfx)(
+        x.shape[0] // 3, x, index, cap, total, idx, pos, np.ascontiguousarray(y1, dt_),
+        np.ascontiguousarray(y2, dt_), np.ascontiguousarray(i1, dt_))
+    return out
+
+
+def pd_inverse_deformation(x, rs, h, dtype=np.float32):
+    sfx, dt_ = _rt(dtype)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    n = x.shape[0] // 3
+    index, cap, total, idx, pos = rs.args(dt_)
+    invF = np.zeros(9 * max(n, 1), dt_)
+    getattr(lib(), "pko_pd_inverse_deformation" + sfx)(n, x, index, cap, total, idx, pos, h, invF)
+    return invF[: 9 * n].reshape(n, 3, 3)
+
+
+def pd_reconstruct(x, rs, byield, nbr_index, nbr_elements, nbr_cap, h, dtype=np.float32):
+    """ElastoplasticityModule::reconstructRestShape: (new CSR RestShape, cleared byield)."""
+    sfx, dt_ = _rt(dtype)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    n = x.shape[0] // 3
+    nbr_index = np.ascontiguousarray(nbr_index, np.int32)
+    nbr_elements = np.ascontiguousarray(nbr_elements, np.int32)
+    nbr_total = _total(nbr_index, nbr_elements, nbr_cap)
+    by = np.array(byield, np.uint8)
+    index, cap, total, idx, pos = rs.args(dt_)
+    sizes = np.zeros(max(n, 1), np.int32)
+    getattr(lib(), "pko_pd_recon_sizes" + sfx)(n, by, nbr_index, nbr_cap, nbr_total, index, cap, total, sizes)
+    sizes = sizes[:n]
+    off = np.zeros(n + 1, np.int64)
+    off[1:] = np.cumsum(sizes)
+    tot = int(off[-1])
+    off32 = np.ascontiguousarray(off[:max(n, 1)], np.int32)
+    invF = pd_inverse_deformation(x, rs, h, dtype).reshape(-1)
+    new_idx = np.zeros(max(tot, 1), np.int32)
+    new_pos = np.zeros(3 * max(tot, 1), dt_)
+    getattr(lib(), "pko_pd_recon_fill" + sfx)(n, x, by, np.ascontiguousarray(invF, dt_), nbr_index, nbr_elements,
+                                               nbr_cap, nbr_total, index, cap, total, idx, pos, off32, new_idx,
+                                               new_pos)
+    return RestShape(off32[:n], 0, tot, new_idx[:max(tot, 1)], new_pos), by
+
+
+def pd_fracture(x, rs, bulk, h, A, B, mu, lam, dtype=np.float32):
+    """FractureModule::applyPlasticity: returns the new bulk stiffness."""
+    sfx, dt_ = _rt(dtype)
+    x = np.ascontiguousarray(x, dt_).reshape(-1)
+    b = np.array(bulk, dt_)
+    index, cap, total, idx, pos = rs.args(dt_)
+    getattr(lib(), "pko_pd_fracture" + sfx)(x.shape[0] // 3, x, index, cap, total, idx, pos, b, h, A, B, mu, lam)
+    return b
+
+
+def drucker_prager(c, phi):
+    """ElastoplasticityModule::computeA/computeB (ElastoplasticityModule.h:53-64),
+    phi as stored by the module (setFrictionAngle divides degrees by 180)."""
+    A = 6.0 * c * np.cos(phi) / (3.0 + np.sin(phi)) / np.sqrt(3.0)
+    B = 2.0 * np.sin(phi) / (3.0 + np.sin(phi)) / np.sqrt(3.0)
+    return float(np.float32(A)), float(np.float32(B))

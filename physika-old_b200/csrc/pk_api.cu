@@ -242,7 +242,8 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
     void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
-                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau, c->tau_hint,
+                    c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau, c->tau_hint, c->pl_y1, c->pl_y2, c->pl_i1, c->pl_yield,
+                    c->pl_invF, c->pl_sizes, c->pl_off, c->pl_rest_idx2, c->pl_rest_pos2,
                     c->hcnt, c->items, c->nitems,
                     c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
@@ -771,15 +772,24 @@ PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const 
         }
         c->pd_cap_n = n;
     }
-    if (bonds > c->pd_cap_bonds) {
-        if (!(regrow(c->pd_rest_idx, (size_t)bonds) && regrow(c->pd_rest_pos, 3 * (size_t)bonds) &&
-              regrow(c->pd_alive, (size_t)bonds) && regrow(c->pd_in, (size_t)bonds))) {
-            c->pd_cap_bonds = 0;
+    if (bonds > c->pd_cap_rest) {
+        if (!(regrow(c->pd_rest_idx, (size_t)bonds) && regrow(c->pd_rest_pos, 3 * (size_t)bonds))) {
+            c->pd_cap_rest = 0;
             return fail(c, PK_ERR_NOMEM, "device allocation of the rest shape failed");
+        }
+        c->pd_cap_rest = bonds;
+    }
+    if (bonds > c->pd_cap_bonds) {
+        if (!(regrow(c->pd_alive, (size_t)bonds) && regrow(c->pd_in, (size_t)bonds))) {
+            c->pd_cap_bonds = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of the bond masks failed");
         }
         c->pd_cap_bonds = bonds;
     }
     c->pd_n = n;
+    c->pd_begun = false;
+    if (c->pl_yield && n > 0 && n <= c->pl_cap_n)  // m_bYield.reset() (ElastoplasticityModule.cu:665)
+        cudaMemsetAsync(c->pl_yield, 0, (size_t)n, (cudaStream_t)stream);
     c->pd_cap = cap;
     c->pd_total = bonds;
     c->pd_horizon = horizon;
@@ -894,6 +904,234 @@ PK_API int pk_pd_rollout_backward_f64(pk_ctx* c, const double* xbar, const doubl
     c->launches = pk::pd_backward_f64(c, xbar, vbar, grad_x0, grad_v0, grad_bulk, (cudaStream_t)stream);
     if (c->launches < 0) return fail(c, PK_ERR_STATE, "no checkpointed double rollout to differentiate");
     return check_launch(c, "pk_pd_rollout_backward_f64");
+}
+
+// ======================================================================
+// ElasticityModule step by step, ElastoplasticityModule, FractureModule
+
+namespace {
+int check_pd(pk_ctx* c, int n)
+{
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    if (n != c->pd_n) return fail(c, PK_ERR_ARG, "particle count differs from pk_pd_init");
+    return PK_OK;
+}
+
+int check_pd_params(pk_ctx* c, const pk_pd_params* p)
+{
+    if (!p) return fail(c, PK_ERR_ARG, "null elasticity parameters");
+    if (!(p->horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
+    if (p->break_stretch > 0.0f) return fail(c, PK_ERR_ARG, "break_stretch must be 0 for step-by-step solves");
+    return PK_OK;
+}
+
+int check_plastic(pk_ctx* c, int n, const float* x, const pk_plastic_params* p)
+{
+    int rc = check_pd(c, n);
+    if (rc) return rc;
+    if (!p) return fail(c, PK_ERR_ARG, "null plasticity parameters");
+    if (!(p->horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    return PK_OK;
+}
+
+// The yield state of ElastoplasticityModule::initializeImpl (m_bYield reset,
+// ElastoplasticityModule.cu:659-668), allocated on first use.
+int ensure_plastic(pk_ctx* c)
+{
+    const int n = c->pd_n;
+    if (n <= c->pl_cap_n && c->pl_y1) return PK_OK;
+    const size_t m = (size_t)std::max(n, 1);
+    if (!(regrow(c->pl_y1, m) && regrow(c->pl_y2, m) && regrow(c->pl_i1, m) && regrow(c->pl_yield, m) &&
+          regrow(c->pl_invF, 9 * m) && regrow(c->pl_sizes, m + 1) && regrow(c->pl_off, m + 1))) {
+        c->pl_cap_n = 0;
+        return fail(c, PK_ERR_NOMEM, "device allocation of the plasticity state failed");
+    }
+    cudaMemset(c->pl_yield, 0, m);
+    cudaMemset(c->pl_y1, 0, sizeof(float) * m);
+    cudaMemset(c->pl_y2, 0, sizeof(float) * m);
+    cudaMemset(c->pl_i1, 0, sizeof(float) * m);
+    c->pl_cap_n = n;
+    return PK_OK;
+}
+}  // namespace
+
+PK_API int pk_pd_compute_inverse_k(pk_ctx* c, float horizon, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    if (!(horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_inverse_k(c, horizon, (cudaStream_t)stream);
+    return check_launch(c, "pk_pd_compute_inverse_k");
+}
+
+PK_API int pk_pd_begin(pk_ctx* c, const float* x, int n, const pk_pd_params* p, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_pd(c, n);
+    if (rc || (rc = check_pd_params(c, p))) return rc;
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_begin(c, x, n, p->horizon, p->mu, p->lambda, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_NOMEM, "device allocation of the projection workspace failed");
+    c->pd_begun = true;
+    return check_launch(c, "pk_pd_begin");
+}
+
+PK_API int pk_pd_enforce(pk_ctx* c, float* x, int n, const pk_pd_params* p, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_pd(c, n);
+    if (rc || (rc = check_pd_params(c, p))) return rc;
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    if (!c->pd_begun) return fail(c, PK_ERR_STATE, "pk_pd_begin has not been called");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_enforce(c, x, n, p->horizon, p->mu, p->lambda, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_STATE, "pk_pd_begin has not been called for this size");
+    return check_launch(c, "pk_pd_enforce");
+}
+
+PK_API int pk_pd_update_velocity(pk_ctx* c, const float* x, float* v, int n, float dt, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_pd(c, n);
+    if (rc) return rc;
+    if (n > 0 && (!x || !v)) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    if (!(dt > 0.0f)) return fail(c, PK_ERR_ARG, "dt must be positive");
+    if (!c->pd_begun) return fail(c, PK_ERR_STATE, "pk_pd_begin has not been called");
+    cudaSetDevice(c->device);
+    c->launches = pk::pd_update_velocity(c, x, v, n, dt, (cudaStream_t)stream);
+    if (c->launches < 0) return fail(c, PK_ERR_STATE, "pk_pd_begin has not been called for this size");
+    return check_launch(c, "pk_pd_update_velocity");
+}
+
+PK_API int pk_pd_rotate_rest_shape(pk_ctx* c, const float* x, int n, float horizon, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_pd(c, n);
+    if (rc) return rc;
+    if (!(horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    cudaSetDevice(c->device);
+    c->launches = pk::pl_rotate(c, x, horizon, (cudaStream_t)stream);
+    return check_launch(c, "pk_pd_rotate_rest_shape");
+}
+
+PK_API int pk_pd_apply_yielding(pk_ctx* c, const float* x, int n, const pk_plastic_params* p, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_plastic(c, n, x, p);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    if ((rc = ensure_plastic(c))) return rc;
+    c->launches = pk::pl_yield(c, x, p, (cudaStream_t)stream);
+    return check_launch(c, "pk_pd_apply_yielding");
+}
+
+PK_API int pk_pd_fracture(pk_ctx* c, const float* x, int n, const pk_plastic_params* p, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_plastic(c, n, x, p);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    c->launches = pk::pl_fracture(c, x, p, (cudaStream_t)stream);
+    return check_launch(c, "pk_pd_fracture");
+}
+
+PK_API int pk_pd_reconstruct_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int* elements,
+                                        int cap, long long total, float horizon, int reconstruct_all,
+                                        pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = check_pd(c, n);
+    if (rc) return rc;
+    if ((rc = check_list(c, n, index, elements, cap, total))) return rc;
+    if (!(horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
+    if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
+    cudaSetDevice(c->device);
+    if ((rc = ensure_plastic(c))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    int l = 0;
+    if (reconstruct_all) l += pk::pl_enable_all(c, st);
+    l += pk::pl_recon_begin(c, x, index, cap, total, horizon, st);
+    int new_total = 0;
+    if (n > 0) {
+        cudaError_t e = cudaMemcpyAsync(&new_total, c->pl_off + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(c, e, "pk_pd_reconstruct_rest_shape");
+    }
+    if (new_total < 0) return fail(c, PK_ERR_ARG, "more than 2^31 rest bonds");
+    if (new_total > c->pl_cap_rest2) {
+        if (!(regrow(c->pl_rest_idx2, (size_t)new_total) && regrow(c->pl_rest_pos2, 3 * (size_t)new_total))) {
+            c->pl_cap_rest2 = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of the reconstructed rest shape failed");
+        }
+        c->pl_cap_rest2 = new_total;
+    }
+    l += pk::pl_recon_fill(c, x, index, elements, cap, total, st);
+    // the new shape becomes the rest shape (CSR); the old buffers are the next spares
+    std::swap(c->pd_rest_idx, c->pl_rest_idx2);
+    std::swap(c->pd_rest_pos, c->pl_rest_pos2);
+    std::swap(c->pd_cap_rest, c->pl_cap_rest2);
+    if (new_total > c->pd_cap_bonds) {
+        if (!(regrow(c->pd_alive, (size_t)new_total) && regrow(c->pd_in, (size_t)new_total))) {
+            c->pd_cap_bonds = 0;
+            return fail(c, PK_ERR_NOMEM, "device allocation of the bond masks failed");
+        }
+        c->pd_cap_bonds = new_total;
+    }
+    if (n > 0) cudaMemcpyAsync(c->pd_index, c->pl_off, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    c->pd_cap = 0;
+    c->pd_total = new_total;
+    l += pk::pl_fill_alive(c, new_total, st);
+    if (n > 0) l += pk::pd_build_incoming(c, st);
+    c->launches = l;
+    return check_launch(c, "pk_pd_reconstruct_rest_shape");
+}
+
+PK_API int pk_pd_get_yield(pk_ctx* c, float* yield_i1, float* yield_j2, float* i1, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    cudaSetDevice(c->device);
+    int rc = ensure_plastic(c);
+    if (rc) return rc;
+    const size_t b = sizeof(float) * (size_t)c->pd_n;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (yield_i1 && b) e = cudaMemcpyAsync(yield_i1, c->pl_y1, b, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && yield_j2 && b) e = cudaMemcpyAsync(yield_j2, c->pl_y2, b, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && i1 && b) e = cudaMemcpyAsync(i1, c->pl_i1, b, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_pd_get_yield");
+    return PK_OK;
+}
+
+PK_API int pk_pd_get_bulk(pk_ctx* c, float* bulk, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    cudaSetDevice(c->device);
+    if (!bulk || c->pd_n == 0) return PK_OK;
+    cudaError_t e = cudaMemcpyAsync(bulk, c->pd_bulk, sizeof(float) * (size_t)c->pd_n, cudaMemcpyDeviceToDevice,
+                                    (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_pd_get_bulk");
+    return PK_OK;
+}
+
+PK_API int pk_pd_rest_layout(pk_ctx* c, int* index, int* cap, long long* total, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (c->pd_n < 0) return fail(c, PK_ERR_STATE, "pk_pd_init has not been called");
+    cudaSetDevice(c->device);
+    if (cap) *cap = c->pd_cap;
+    if (total) *total = c->pd_total;
+    if (index && c->pd_n > 0) {
+        cudaError_t e = cudaMemcpyAsync(index, c->pd_index, sizeof(int) * (size_t)c->pd_n, cudaMemcpyDeviceToDevice,
+                                        (cudaStream_t)stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "pk_pd_rest_layout");
+    }
+    return PK_OK;
 }
 
 PK_API int pk_pd_get_rest_shape(pk_ctx* c, int* rest_idx, float* rest_pos, float* inv_k, pk_stream stream)

@@ -93,8 +93,23 @@ struct pk_ctx {
     float* pd_delta = nullptr;
     float* pd_w = nullptr;
     float pd_horizon = 0.0f;
-    long long pd_cap_bonds = 0;
+    long long pd_cap_bonds = 0;    // capacity of pd_alive and pd_in
+    long long pd_cap_rest = 0;     // capacity of pd_rest_idx / pd_rest_pos
     int pd_cap_n = 0;
+    // ElastoplasticityModule state (n per array) and the spare rest-shape
+    // buffers a reconstruction fills before they are swapped in
+    int pl_cap_n = 0;
+    float* pl_y1 = nullptr;         // m_yiled_I1
+    float* pl_y2 = nullptr;         // m_yield_J2
+    float* pl_i1 = nullptr;         // m_I1
+    unsigned char* pl_yield = nullptr;  // m_bYield
+    float* pl_invF = nullptr;       // m_invF, 9 per particle
+    int* pl_sizes = nullptr;        // n + 1
+    int* pl_off = nullptr;          // n + 1
+    int* pl_rest_idx2 = nullptr;
+    float* pl_rest_pos2 = nullptr;
+    long long pl_cap_rest2 = 0;
+    bool pd_begun = false;          // pk_pd_begin has run since pk_pd_init
     int* pd_in_cnt = nullptr;   // incoming bonds per particle (n + 1)
     int* pd_in_off = nullptr;   // their CSR offsets (n + 1)
     int2* pd_in = nullptr;      // (source particle, bond slot) of every incoming bond

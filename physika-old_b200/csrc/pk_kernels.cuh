@@ -54,6 +54,20 @@ int boundary_jitter(float* out, int n, cudaStream_t st);
 
 // pk_pd_adj.cu
 int pd_build_incoming(pk_ctx* c, cudaStream_t st);
+int pd_inverse_k(pk_ctx* c, float horizon, cudaStream_t st);
+int pd_begin(pk_ctx* c, const float* x, int n, float horizon, float mu, float lambda, cudaStream_t st);
+int pd_enforce(pk_ctx* c, float* x, int n, float horizon, float mu, float lambda, cudaStream_t st);
+int pd_update_velocity(pk_ctx* c, const float* x, float* v, int n, float dt, cudaStream_t st);
+// pk_plastic.cu
+int pl_rotate(pk_ctx* c, const float* x, float h, cudaStream_t st);
+int pl_yield(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t st);
+int pl_fracture(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t st);
+int pl_enable_all(pk_ctx* c, cudaStream_t st);
+int pl_recon_begin(pk_ctx* c, const float* x, const int* nindex, int ncap, long long ntotal, float h,
+                   cudaStream_t st);
+int pl_recon_fill(pk_ctx* c, const float* x, const int* nindex, const int* nelements, int ncap, long long ntotal,
+                  cudaStream_t st);
+int pl_fill_alive(pk_ctx* c, long long bonds, cudaStream_t st);
 int pd_project_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, float lambda, int iterations,
                      float dt, cudaStream_t st);
 int pd_rollout_f32(pk_ctx* c, float* x, float* v, int n, const float g[3], const pk_pd_params* p, int steps,

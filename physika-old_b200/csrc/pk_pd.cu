@@ -1,9 +1,10 @@
 // pk_pd.cu -- ElasticityModule (projective peridynamics).
 //
-// The rest shape (bond list + rest positions) is frozen at initialisation
-// (ElasticityModule::resetRestShape, ElasticityModule.cu:496-517), so K^-1 is
-// computed once here; the reference recomputes the same matrix every step
-// (solveElasticity -> computeInverseK, :404-411).  Each projection iteration
+// The rest shape (bond list + rest positions) is set at initialisation
+// (ElasticityModule::resetRestShape, ElasticityModule.cu:496-517) and K^-1 is
+// computed with it; the reference recomputes the same matrix every step
+// (solveElasticity -> computeInverseK, :404-411), which pk_pd_compute_inverse_k
+// does where plasticity moves the rest shape.  Each projection iteration
 // is EM_EnforceElasticity (:123-242) + K_UpdatePosition (:281-292).
 #include "pk_kernels.cuh"
 #include "pk_pd_common.cuh"
@@ -39,41 +40,6 @@ __global__ void __launch_bounds__(256)
             rpos[3 * a0 + 2] = x[3 * j + 2];
         }
     }
-}
-
-// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations in double.
-__device__ void jacobi3(double A[3][3], double Q[3][3], double w[3])
-{
-    for (int p = 0; p < 3; ++p)
-        for (int q = 0; q < 3; ++q) Q[p][q] = (p == q) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 60; ++sweep) {
-        double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
-        if (off < 1e-300) break;
-        for (int p = 0; p < 2; ++p)
-            for (int q = p + 1; q < 3; ++q) {
-                double apq = A[p][q];
-                if (fabs(apq) < 1e-300) continue;
-                double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-                for (int r = 0; r < 3; ++r) {
-                    double arp = A[r][p], arq = A[r][q];
-                    A[r][p] = c * arp - s * arq;
-                    A[r][q] = s * arp + c * arq;
-                }
-                for (int r = 0; r < 3; ++r) {
-                    double apr = A[p][r], aqr = A[q][r];
-                    A[p][r] = c * apr - s * aqr;
-                    A[q][r] = s * apr + c * aqr;
-                }
-                for (int r = 0; r < 3; ++r) {
-                    double qrp = Q[r][p], qrq = Q[r][q];
-                    Q[r][p] = c * qrp - s * qrq;
-                    Q[r][q] = s * qrp + c * qrq;
-                }
-            }
-    }
-    for (int p = 0; p < 3; ++p) w[p] = A[p][p];
 }
 
 // EM_PrecomputeShape (ElasticityModule.cu:21-116): weighted second moment of
@@ -172,6 +138,15 @@ int pd_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int*
     if (bonds > 0)
         k_fill_u8<<<(unsigned)((bonds + 255) / 256), 256, 0, st>>>(c->pd_alive, bonds, 1);
     return 5;
+}
+
+int pd_inverse_k(pk_ctx* c, float horizon, cudaStream_t st)
+{
+    const int n = c->pd_n;
+    if (n <= 0) return 0;
+    k_pd_invk<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_pos,
+                                                          horizon, c->pd_invK);
+    return 1;
 }
 
 int pd_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, float lambda,

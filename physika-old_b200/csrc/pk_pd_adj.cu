@@ -764,6 +764,43 @@ int pd_project_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float 
     return l + 1;
 }
 
+// The projection one step at a time (pk_pd_begin / pk_pd_enforce /
+// pk_pd_update_velocity): x_old and the bond weights are kept in the float
+// workspace between the calls.
+int pd_begin(pk_ctx* c, const float* x, int n, float horizon, float mu, float lambda, cudaStream_t st)
+{
+    PdWork<float>* w = ensure_work<float>(c, n);
+    if (!w) return -1;
+    if (n <= 0) return 0;
+    const PdBonds B = bonds_of(c, horizon, mu, lambda);
+    k_pd_W<float, float><<<pd_groups_blocks(n), kPdBlock, 0, st>>>(B, c->pd_bulk, w->W);
+    cudaMemcpyAsync(w->xold, x, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    return 1;
+}
+
+int pd_enforce(pk_ctx* c, float* x, int n, float horizon, float mu, float lambda, cudaStream_t st)
+{
+    PdWork<float>* w = work_of<float>(c);
+    if (!w || w->cap_n < n) return -1;
+    if (n <= 0) return 0;
+    const PdBonds B = bonds_of(c, horizon, mu, lambda);
+    const unsigned nb128 = pd_groups_blocks(n);
+    k_pd_F<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->F, nullptr);
+    k_pd_P<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->xold, w->F, c->pd_bulk, w->W, w->xa);
+    cudaMemcpyAsync(x, w->xa, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    return 2;
+}
+
+int pd_update_velocity(pk_ctx* c, const float* x, float* v, int n, float dt, cudaStream_t st)
+{
+    PdWork<float>* w = work_of<float>(c);
+    if (!w || w->cap_n < n) return -1;
+    if (n <= 0) return 0;
+    const long long m3 = 3LL * n;
+    k_pd_vel<float><<<(unsigned)((m3 + 255) / 256), 256, 0, st>>>(m3, v, x, w->xold, dt);
+    return 1;
+}
+
 template <class R>
 static int rollout(pk_ctx* c, R* x, R* v, const R* bulk_in, int n, const R g[3], const pk_pd_params* p, int steps,
                    int every, cudaStream_t st)

@@ -35,4 +35,39 @@ __device__ __forceinline__ float corr_wrr(float r, float h)
     return q * smooth_w(r, h) / (h * h);
 }
 
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations in double.
+__device__ inline void jacobi3(double A[3][3], double Q[3][3], double w[3])
+{
+    for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) Q[p][q] = (p == q) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
+        if (off < 1e-300) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                double apq = A[p][q];
+                if (fabs(apq) < 1e-300) continue;
+                double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int r = 0; r < 3; ++r) {
+                    double arp = A[r][p], arq = A[r][q];
+                    A[r][p] = c * arp - s * arq;
+                    A[r][q] = s * arp + c * arq;
+                }
+                for (int r = 0; r < 3; ++r) {
+                    double apr = A[p][r], aqr = A[q][r];
+                    A[p][r] = c * apr - s * aqr;
+                    A[q][r] = s * apr + c * aqr;
+                }
+                for (int r = 0; r < 3; ++r) {
+                    double qrp = Q[r][p], qrq = Q[r][q];
+                    Q[r][p] = c * qrp - s * qrq;
+                    Q[r][q] = s * qrp + c * qrq;
+                }
+            }
+    }
+    for (int p = 0; p < 3; ++p) w[p] = A[p][p];
+}
+
 }  // namespace pk

@@ -21,6 +21,9 @@ EXPORTED = [
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
     "pk_pbf_step_batched",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
+    "pk_pd_compute_inverse_k", "pk_pd_begin", "pk_pd_enforce", "pk_pd_update_velocity",
+    "pk_pd_rotate_rest_shape", "pk_pd_apply_yielding", "pk_pd_reconstruct_rest_shape", "pk_pd_fracture",
+    "pk_pd_get_yield", "pk_pd_get_bulk", "pk_pd_rest_layout",
     "pk_pd_rollout", "pk_pd_rollout_backward", "pk_pd_rollout_f64", "pk_pd_rollout_backward_f64",
     "pk_noalloc_max_particles", "pk_pbd_solve_noalloc",
 ]
@@ -52,6 +55,11 @@ class PbfParams(ctypes.Structure):
 class PdParams(ctypes.Structure):
     _fields_ = [("horizon", ctypes.c_float), ("mu", ctypes.c_float), ("lambda_", ctypes.c_float),
                 ("iterations", ctypes.c_int), ("dt", ctypes.c_float), ("break_stretch", ctypes.c_float)]
+
+
+class PlasticParams(ctypes.Structure):
+    _fields_ = [("horizon", ctypes.c_float), ("mu", ctypes.c_float), ("lambda_", ctypes.c_float),
+                ("A", ctypes.c_float), ("B", ctypes.c_float)]
 
 
 _lib = None
@@ -94,6 +102,17 @@ def load():
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
         "pk_pd_get_rest_shape": ([P, P, P, P, P], I),
+        "pk_pd_compute_inverse_k": ([P, F, P], I),
+        "pk_pd_begin": ([P, P, I, ctypes.POINTER(PdParams), P], I),
+        "pk_pd_enforce": ([P, P, I, ctypes.POINTER(PdParams), P], I),
+        "pk_pd_update_velocity": ([P, P, P, I, F, P], I),
+        "pk_pd_rotate_rest_shape": ([P, P, I, F, P], I),
+        "pk_pd_apply_yielding": ([P, P, I, ctypes.POINTER(PlasticParams), P], I),
+        "pk_pd_reconstruct_rest_shape": ([P, P, I, P, P, I, LL, F, I, P], I),
+        "pk_pd_fracture": ([P, P, I, ctypes.POINTER(PlasticParams), P], I),
+        "pk_pd_get_yield": ([P, P, P, P, P], I),
+        "pk_pd_get_bulk": ([P, P, P], I),
+        "pk_pd_rest_layout": ([P, P, ctypes.POINTER(I), ctypes.POINTER(LL), P], I),
         "pk_pd_rollout": ([P, P, P, I, ctypes.POINTER(F * 3), ctypes.POINTER(PdParams), I, I, P], I),
         "pk_pd_rollout_backward": ([P, P, P, P, P, P, P], I),
         "pk_pd_rollout_f64": ([P, P, P, P, I, ctypes.POINTER(ctypes.c_double * 3), ctypes.POINTER(PdParams),
@@ -332,6 +351,57 @@ class Context:
         fn = self.L.pk_pd_rollout_backward_f64 if xbar.dtype == torch.float64 else self.L.pk_pd_rollout_backward
         self._check(fn(self.h, _ptr(xbar), _ptr(vbar), _ptr(gx), _ptr(gv), _ptr(gb), _stream()))
         return gx, gv, gb
+
+    # ---- ElasticityModule step by step, ElastoplasticityModule, FractureModule
+    def pd_compute_inverse_k(self, horizon):
+        self._check(self.L.pk_pd_compute_inverse_k(self.h, float(horizon), _stream()))
+
+    def pd_begin(self, x, horizon, mu=0.05, lam=0.1, dt=1e-3):
+        p = PdParams(float(horizon), float(mu), float(lam), 1, float(dt), 0.0)
+        self._check(self.L.pk_pd_begin(self.h, _ptr(x), x.shape[0], ctypes.byref(p), _stream()))
+
+    def pd_enforce(self, x, horizon, mu=0.05, lam=0.1, dt=1e-3):
+        p = PdParams(float(horizon), float(mu), float(lam), 1, float(dt), 0.0)
+        self._check(self.L.pk_pd_enforce(self.h, _ptr(x), x.shape[0], ctypes.byref(p), _stream()))
+
+    def pd_update_velocity(self, x, v, dt):
+        self._check(self.L.pk_pd_update_velocity(self.h, _ptr(x), _ptr(v), x.shape[0], float(dt), _stream()))
+
+    def pd_rotate_rest_shape(self, x, horizon):
+        self._check(self.L.pk_pd_rotate_rest_shape(self.h, _ptr(x), x.shape[0], float(horizon), _stream()))
+
+    def pd_apply_yielding(self, x, horizon, A, B, mu=0.05, lam=0.1):
+        p = PlasticParams(float(horizon), float(mu), float(lam), float(A), float(B))
+        self._check(self.L.pk_pd_apply_yielding(self.h, _ptr(x), x.shape[0], ctypes.byref(p), _stream()))
+
+    def pd_fracture(self, x, horizon, A, B, mu=0.05, lam=0.1):
+        p = PlasticParams(float(horizon), float(mu), float(lam), float(A), float(B))
+        self._check(self.L.pk_pd_fracture(self.h, _ptr(x), x.shape[0], ctypes.byref(p), _stream()))
+
+    def pd_reconstruct_rest_shape(self, x, index, elements, cap, total, horizon, reconstruct_all=False):
+        self._check(self.L.pk_pd_reconstruct_rest_shape(self.h, _ptr(x), x.shape[0], _ptr(index), _ptr(elements),
+                                                        int(cap), int(total), float(horizon),
+                                                        int(bool(reconstruct_all)), _stream()))
+
+    def pd_get_yield(self, n):
+        import torch
+        out = [torch.zeros(n, device="cuda") for _ in range(3)]
+        self._check(self.L.pk_pd_get_yield(self.h, *[_ptr(t) for t in out], _stream()))
+        return out
+
+    def pd_get_bulk(self, n):
+        import torch
+        b = torch.zeros(n, device="cuda")
+        self._check(self.L.pk_pd_get_bulk(self.h, _ptr(b), _stream()))
+        return b
+
+    def pd_rest_layout(self, n):
+        """(index tensor, cap, total) of the current rest shape."""
+        import torch
+        idx = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+        cap, tot = ctypes.c_int(), ctypes.c_longlong()
+        self._check(self.L.pk_pd_rest_layout(self.h, _ptr(idx), ctypes.byref(cap), ctypes.byref(tot), _stream()))
+        return idx[:n], cap.value, tot.value
 
     def pd_get_rest_shape(self, rest_idx=None, rest_pos=None, inv_k=None):
         self._check(self.L.pk_pd_get_rest_shape(self.h, _ptr(rest_idx), _ptr(rest_pos), _ptr(inv_k),
