@@ -1,6 +1,8 @@
 // ParticleModules.cpp -- module bodies: every compute goes through the C ABI.
 #include "ParticleModules.h"
 
+#include <cmath>
+
 #include <map>
 
 namespace PhysIKA {
@@ -349,17 +351,46 @@ void ElasticityModule<TDataType>::computeMaterialStiffness()
 }
 
 template <typename TDataType>
+pk_pd_params ElasticityModule<TDataType>::stepParams()
+{
+    return pk_pd_params{this->inHorizon()->getValue(), m_mu.getValue(), m_lambda.getValue(), 1,
+                        this->getParent()->getDt(), 0};
+}
+
+template <typename TDataType>
+void ElasticityModule<TDataType>::beginSolve()
+{
+    pk_ctx* c = contextOf(this);
+    pk_pd_params p = stepParams();
+    pkCheck(pk_pd_begin(c, F(this->inPosition()->getValue()), (int)this->inPosition()->getElementCount(), &p, 0),
+            c, "ElasticityModule::solveElasticity");
+}
+
+template <typename TDataType>
+void ElasticityModule<TDataType>::computeInverseK()
+{
+    pk_ctx* c = contextOf(this);
+    pkCheck(pk_pd_compute_inverse_k(c, this->inHorizon()->getValue(), 0), c, "ElasticityModule::computeInverseK");
+}
+
+template <typename TDataType>
 void ElasticityModule<TDataType>::enforceElasticity()
 {
-    // One projection iteration (EM_EnforceElasticity + K_UpdatePosition) is
-    // part of pk_pd_solve; a standalone call runs a single-iteration solve.
+    // EM_EnforceElasticity + K_UpdatePosition (ElasticityModule.cu:123-292)
     pk_ctx* c = contextOf(this);
-    pk_pd_params p{this->inHorizon()->getValue(), m_mu.getValue(), m_lambda.getValue(), 1,
-                   this->getParent()->getDt(), m_breakStretch};
-    DeviceArray<Coord> scratch((int)this->inPosition()->getElementCount());
-    pkCheck(pk_pd_solve(c, F(this->inPosition()->getValue()), F(scratch), scratch.size(), &p, 0), c,
-            "ElasticityModule::enforceElasticity");
-    scratch.release();
+    pk_pd_params p = stepParams();
+    pkCheck(pk_pd_enforce(c, F(this->inPosition()->getValue()), (int)this->inPosition()->getElementCount(), &p, 0),
+            c, "ElasticityModule::enforceElasticity");
+}
+
+template <typename TDataType>
+void ElasticityModule<TDataType>::updateVelocity()
+{
+    // K_UpdateVelocity (ElasticityModule.cu:295-306)
+    pk_ctx* c = contextOf(this);
+    pkCheck(pk_pd_update_velocity(c, F(this->inPosition()->getValue()), F(this->inVelocity()->getValue()),
+                                  (int)this->inPosition()->getElementCount(), this->getParent()->getDt(), 0),
+            c, "ElasticityModule::updateVelocity");
 }
 
 template <typename TDataType>
@@ -379,6 +410,136 @@ bool ElasticityModule<TDataType>::constrain()
 {
     this->solveElasticity();
     return true;
+}
+
+// ====================================================== ElastoplasticityModule
+
+template <typename TDataType>
+ElastoplasticityModule<TDataType>::ElastoplasticityModule()
+{
+    // ElastoplasticityModule.cu:13-25 (m_c 0.001, m_phi 60/180, no full
+    // reconstruction, incompressible)
+}
+
+template <typename TDataType>
+typename TDataType::Real ElastoplasticityModule<TDataType>::computeA()
+{
+    const Real phi = m_phi.getValue();
+    return Real(6.0) * m_c.getValue() * std::cos(phi) / (3.0f + std::sin(phi)) / std::sqrt(3.0f);
+}
+
+template <typename TDataType>
+typename TDataType::Real ElastoplasticityModule<TDataType>::computeB()
+{
+    const Real phi = m_phi.getValue();
+    return Real(2.0f) * std::sin(phi) / (3.0f + std::sin(phi)) / std::sqrt(3.0f);
+}
+
+template <typename TDataType>
+pk_plastic_params ElastoplasticityModule<TDataType>::plasticParams()
+{
+    return pk_plastic_params{this->inHorizon()->getValue(), this->m_mu.getValue(), this->m_lambda.getValue(),
+                             computeA(), computeB()};
+}
+
+template <typename TDataType>
+bool ElastoplasticityModule<TDataType>::initializeImpl()
+{
+    // ElastoplasticityModule.cu:659-683: the inner DensityPBD on the body's
+    // horizon, positions, velocities and neighbour list
+    m_pbdModule = std::make_shared<DensityPBD<TDataType>>();
+    this->inHorizon()->connect(m_pbdModule->varSmoothingLength());
+    this->inPosition()->connect(m_pbdModule->inPosition());
+    this->inVelocity()->connect(m_pbdModule->inVelocity());
+    this->inNeighborhood()->connect(m_pbdModule->inNeighborIndex());
+    m_pbdModule->setParent(this->getParent());
+    m_pbdModule->initialize();
+    return ElasticityModule<TDataType>::initializeImpl();
+}
+
+template <typename TDataType>
+void ElastoplasticityModule<TDataType>::solveElasticity()
+{
+    // ElastoplasticityModule.cu:240-262
+    this->beginSolve();
+    this->computeInverseK();
+    m_pbdModule->varIterationNumber()->setValue(1);
+    const int total = this->getIterationNumber();
+    for (int iter = 0; iter < total; ++iter) {
+        this->enforceElasticity();
+        if (m_incompressible.getValue()) m_pbdModule->constrain();
+    }
+    this->updateVelocity();
+}
+
+template <typename TDataType>
+void ElastoplasticityModule<TDataType>::rotateRestShape()
+{
+    pk_ctx* c = contextOf(this);
+    pkCheck(pk_pd_rotate_rest_shape(c, F(this->inPosition()->getValue()), (int)this->inPosition()->getElementCount(),
+                                    this->inHorizon()->getValue(), 0),
+            c, "ElastoplasticityModule::rotateRestShape");
+}
+
+template <typename TDataType>
+void ElastoplasticityModule<TDataType>::applyYielding()
+{
+    pk_ctx* c = contextOf(this);
+    pk_plastic_params p = plasticParams();
+    pkCheck(pk_pd_apply_yielding(c, F(this->inPosition()->getValue()), (int)this->inPosition()->getElementCount(),
+                                 &p, 0),
+            c, "ElastoplasticityModule::applyYielding");
+}
+
+template <typename TDataType>
+void ElastoplasticityModule<TDataType>::reconstructRestShape()
+{
+    auto& nbr = this->inNeighborhood()->getValue();
+    pk_ctx* c = contextOf(this);
+    pkCheck(pk_pd_reconstruct_rest_shape(c, F(this->inPosition()->getValue()),
+                                         (int)this->inPosition()->getElementCount(), nbr.getIndex().getDataPtr(),
+                                         nbr.getElements().getDataPtr(), nbr.getNeighborLimit(), nbr.total(),
+                                         this->inHorizon()->getValue(),
+                                         m_reconstuct_all_neighborhood.getValue() ? 1 : 0, 0),
+            c, "ElastoplasticityModule::reconstructRestShape");
+}
+
+template <typename TDataType>
+void ElastoplasticityModule<TDataType>::applyPlasticity()
+{
+    // ElastoplasticityModule.cu:264-271
+    this->rotateRestShape();
+    this->computeMaterialStiffness();
+    this->applyYielding();
+    this->reconstructRestShape();
+}
+
+template <typename TDataType>
+bool ElastoplasticityModule<TDataType>::constrain()
+{
+    this->solveElasticity();
+    this->applyPlasticity();
+    return true;
+}
+
+template <typename TDataType>
+FractureModule<TDataType>::FractureModule()
+{
+    // FractureModule.cu:7-13
+    this->setCohesion(typename TDataType::Real(0.001));
+    this->setIterationNumber(10);
+}
+
+template <typename TDataType>
+void FractureModule<TDataType>::applyPlasticity()
+{
+    // FractureModule.cu:107-128; the context's stiffness is copied back into m_bulkCoefs
+    pk_ctx* c = contextOf(this);
+    pk_plastic_params p = this->plasticParams();
+    pkCheck(pk_pd_fracture(c, F(this->inPosition()->getValue()), (int)this->inPosition()->getElementCount(), &p, 0),
+            c, "FractureModule::applyPlasticity");
+    if (this->m_bulkCoefs.size() > 0)
+        pkCheck(pk_pd_get_bulk(c, this->m_bulkCoefs.getDataPtr(), 0), c, "FractureModule::applyPlasticity");
 }
 
 // =========================================================== ImplicitViscosity
@@ -605,6 +766,90 @@ void ParticleElasticBody<TDataType>::setElasticitySolver(std::shared_ptr<Elastic
     this->addConstraintModule(solver);
 }
 
+// =================================================== ParticleElastoplasticBody
+
+template <typename TDataType>
+ParticleElastoplasticBody<TDataType>::ParticleElastoplasticBody(std::string name)
+    : ParticleSystem<TDataType>(std::move(name))
+{
+    // ParticleElastoplasticBody.cpp:20-63 (surface mesh and its mapping left out)
+    m_integrator = this->template setNumericalIntegrator<ParticleIntegrator<TDataType>>("integrator");
+    this->currentPosition()->connect(m_integrator->inPosition());
+    this->currentVelocity()->connect(m_integrator->inVelocity());
+    this->currentForce()->connect(m_integrator->inForceDensity());
+
+    m_nbrQuery = this->template addComputeModule<NeighborQuery<TDataType>>("neighborhood");
+    m_horizon.connect(m_nbrQuery->inRadius());
+    this->currentPosition()->connect(m_nbrQuery->inPosition());
+
+    auto plasticity = this->template addConstraintModule<ElastoplasticityModule<TDataType>>("elastoplasticity");
+    this->currentPosition()->connect(plasticity->inPosition());
+    this->currentVelocity()->connect(plasticity->inVelocity());
+    m_nbrQuery->outNeighborhood()->connect(plasticity->inNeighborhood());
+    m_horizon.connect(plasticity->inHorizon());
+
+    m_pbdModule = this->template addConstraintModule<DensityPBD<TDataType>>("pbd");
+    m_horizon.connect(m_pbdModule->varSmoothingLength());
+    this->currentPosition()->connect(m_pbdModule->inPosition());
+    this->currentVelocity()->connect(m_pbdModule->inVelocity());
+    m_nbrQuery->outNeighborhood()->connect(m_pbdModule->inNeighborIndex());
+
+    m_visModule = this->template addConstraintModule<ImplicitViscosity<TDataType>>("viscosity");
+    m_visModule->setViscosity(Real(1));
+    m_horizon.connect(&m_visModule->m_smoothingLength);
+    this->currentPosition()->connect(&m_visModule->m_position);
+    this->currentVelocity()->connect(&m_visModule->m_velocity);
+    m_nbrQuery->outNeighborhood()->connect(&m_visModule->m_neighborhood);
+}
+
+template <typename TDataType>
+std::shared_ptr<ElastoplasticityModule<TDataType>> ParticleElastoplasticBody<TDataType>::getElastoplasticitySolver()
+{
+    return this->template getModule<ElastoplasticityModule<TDataType>>("elastoplasticity");
+}
+
+template <typename TDataType>
+void ParticleElastoplasticBody<TDataType>::setElastoplasticitySolver(
+    std::shared_ptr<ElastoplasticityModule<TDataType>> solver)
+{
+    // ParticleElastoplasticBody.cpp:135-150
+    auto module = getElastoplasticitySolver();
+    if (module) this->deleteModule(module);
+    this->currentPosition()->connect(solver->inPosition());
+    this->currentVelocity()->connect(solver->inVelocity());
+    m_nbrQuery->outNeighborhood()->connect(solver->inNeighborhood());
+    m_horizon.connect(solver->inHorizon());
+    solver->setName("elastoplasticity");
+    this->addConstraintModule(solver);
+}
+
+template <typename TDataType>
+bool ParticleElastoplasticBody<TDataType>::initialize()
+{
+    // ParticleElastoplasticBody.cpp:106-112: the list first, then the modules
+    if (!m_nbrQuery->initialize()) return false;
+    m_nbrQuery->compute();
+    auto plasticity = getElastoplasticitySolver();
+    return m_integrator->initialize() && plasticity->initialize() && m_pbdModule->initialize() &&
+           m_visModule->initialize();
+}
+
+template <typename TDataType>
+void ParticleElastoplasticBody<TDataType>::advance(float dt)
+{
+    // ParticleElastoplasticBody.cpp:73-91
+    (void)dt;
+    auto module = getElastoplasticitySolver();
+    m_integrator->begin();
+    m_integrator->integrate();
+    m_nbrQuery->compute();
+    module->solveElasticity();
+    m_nbrQuery->compute();
+    module->applyPlasticity();
+    m_visModule->constrain();
+    m_integrator->end();
+}
+
 template <typename TDataType>
 void StaticBoundary<TDataType>::loadCube(Coord lo, Coord hi, Real distance, bool bOutBoundary)
 {
@@ -627,6 +872,9 @@ template class DensityPBD<DataType3f>;
 template class ParticleIntegrator<DataType3f>;
 template class ElasticityModule<DataType3f>;
 template class ImplicitViscosity<DataType3f>;
+template class ElastoplasticityModule<DataType3f>;
+template class FractureModule<DataType3f>;
+template class ParticleElastoplasticBody<DataType3f>;
 template class BoundaryConstraint<DataType3f>;
 template class PositionBasedFluidModel<DataType3f>;
 template class ParticleSystem<DataType3f>;

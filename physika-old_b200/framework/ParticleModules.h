@@ -139,9 +139,17 @@ public:
 
 protected:
     bool initializeImpl() override;
+    // ElasticityModule.cu:390-421: K^-1 of the current rest shape, one
+    // projection iteration against the positions saved by beginSolve(), and
+    // v += (x - x_old)/dt.  beginSolve() is the Function1Pt::copy of
+    // m_position_old at the top of solveElasticity.
+    void beginSolve();
+    void computeInverseK();
     virtual void enforceElasticity();
+    void updateVelocity();
     // Subclasses set m_bulkCoefs here (the reference initialises it to 1).
     virtual void computeMaterialStiffness();
+    pk_pd_params stepParams();
 
     VarField<Real> m_mu{Real(0.05)};
     VarField<Real> m_lambda{Real(0.1)};
@@ -150,6 +158,56 @@ protected:
 private:
     VarField<int> m_iterNum{10};
     Real m_breakStretch = 0;
+};
+
+// ElastoplasticityModule (Dynamics/ParticleSystem/ElastoplasticityModule.h:18-80):
+// projective peridynamics with a one-iteration DensityPBD after each
+// projection, then plasticity on the rest shape (rotation, Drucker-Prager
+// yielding, reconstruction).
+template <typename TDataType>
+class ElastoplasticityModule : public ElasticityModule<TDataType> {
+public:
+    typedef typename TDataType::Real Real;
+    typedef typename TDataType::Coord Coord;
+
+    ElastoplasticityModule();
+    ~ElastoplasticityModule() override = default;
+
+    bool constrain() override;
+    void solveElasticity() override;
+    virtual void applyPlasticity();
+    void applyYielding();
+    void rotateRestShape();
+    void reconstructRestShape();
+
+    void setCohesion(Real c) { m_c.setValue(c); }
+    void setFrictionAngle(Real phi) { m_phi.setValue(phi / 180); }  // stored as the reference stores it
+    void enableFullyReconstruction() { m_reconstuct_all_neighborhood.setValue(true); }
+    void disableFullyReconstruction() { m_reconstuct_all_neighborhood.setValue(false); }
+    void enableIncompressibility() { m_incompressible.setValue(true); }
+    void disableIncompressibility() { m_incompressible.setValue(false); }
+
+protected:
+    bool initializeImpl() override;
+    Real computeA();
+    Real computeB();
+    pk_plastic_params plasticParams();
+
+private:
+    VarField<Real> m_c{Real(0.001)};
+    VarField<Real> m_phi{Real(60.0 / 180.0)};
+    VarField<bool> m_reconstuct_all_neighborhood{false};
+    VarField<bool> m_incompressible{true};
+    std::shared_ptr<DensityPBD<TDataType>> m_pbdModule;
+};
+
+// FractureModule (Dynamics/ParticleSystem/FractureModule.h:8-20): the same
+// solve; particles past the yield limit lose their bulk stiffness.
+template <typename TDataType>
+class FractureModule : public ElastoplasticityModule<TDataType> {
+public:
+    FractureModule();
+    void applyPlasticity() override;
 };
 
 // ImplicitViscosity (Dynamics/ParticleSystem/ImplicitViscosity.h:9-46): the
@@ -280,6 +338,27 @@ public:
 
 private:
     VarField<Real> m_horizon{Real(0.0085)};
+};
+
+// ParticleElastoplasticBody (ParticleElastoplasticBody.cpp:20-91): integrate,
+// query, solveElasticity, query again, applyPlasticity, ImplicitViscosity.
+template <typename TDataType>
+class ParticleElastoplasticBody : public ParticleSystem<TDataType> {
+public:
+    typedef typename TDataType::Real Real;
+    explicit ParticleElastoplasticBody(std::string name = "default");
+    bool initialize() override;
+    void advance(float dt) override;
+    void setElastoplasticitySolver(std::shared_ptr<ElastoplasticityModule<TDataType>> solver);
+    std::shared_ptr<ElastoplasticityModule<TDataType>> getElastoplasticitySolver();
+    VarField<Real>* varHorizon() { return &m_horizon; }
+
+private:
+    VarField<Real> m_horizon{Real(0.0085)};
+    std::shared_ptr<ParticleIntegrator<TDataType>> m_integrator;
+    std::shared_ptr<NeighborQuery<TDataType>> m_nbrQuery;
+    std::shared_ptr<DensityPBD<TDataType>> m_pbdModule;
+    std::shared_ptr<ImplicitViscosity<TDataType>> m_visModule;
 };
 
 // StaticBoundary::advance (StaticBoundary.cpp:45-59): constrain every

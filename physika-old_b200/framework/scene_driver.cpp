@@ -158,4 +158,47 @@ __attribute__((visibility("default"))) int pkf_elastic_run(const float* x, const
     }
 }
 
+// An elastoplastic body: ParticleElastoplasticBody (ParticleElastoplasticBody.cpp:20-91)
+// with the given horizon, gravity (0, -9.8, 0) and `steps` frames; its solver
+// is an ElastoplasticityModule with cohesion c and friction angle phi (degrees,
+// setFrictionAngle), or a FractureModule when `fracture` is non-zero, and
+// enableFullyReconstruction when `reconstruct_all` is.  Host arrays as
+// pkf_fluid_run.
+__attribute__((visibility("default"))) int pkf_elastoplastic_run(const float* x, const float* v, int n,
+                                                                 const float lo[3], const float hi[3], float horizon,
+                                                                 float dt, int fracture, float cohesion,
+                                                                 float friction_deg, int reconstruct_all, int steps,
+                                                                 float* x_out, float* v_out)
+{
+    try {
+        SceneGraph& scene = SceneGraph::getInstance();
+        scene.setLowerBound(Vector3f(lo[0], lo[1], lo[2]));
+        scene.setUpperBound(Vector3f(hi[0], hi[1], hi[2]));
+        scene.setGravity(Vector3f(0.0f, -9.8f, 0.0f));
+        auto body = std::make_shared<ParticleElastoplasticBody<DataType3f>>("plastic");
+        body->setDt(dt);
+        body->varHorizon()->setValue(horizon);
+        std::shared_ptr<ElastoplasticityModule<DataType3f>> solver;
+        if (fracture)
+            solver = std::make_shared<FractureModule<DataType3f>>();
+        else
+            solver = std::make_shared<ElastoplasticityModule<DataType3f>>();
+        solver->setCohesion(cohesion);
+        solver->setFrictionAngle(friction_deg);
+        if (reconstruct_all) solver->enableFullyReconstruction();
+        body->setElastoplasticitySolver(solver);
+        body->setParticles(to_coords(x, n), to_coords(v, n));
+        if (!body->initialize()) return 1;
+        for (int s = 0; s < steps; ++s) body->advance(dt);
+        std::vector<Vector3f> pos, vel;
+        body->getParticles(pos, vel);
+        from_coords(pos, x_out);
+        from_coords(vel, v_out);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "pkf_elastoplastic_run: %s\n", e.what());
+        return 2;
+    }
+}
+
 }  // extern "C"

@@ -119,3 +119,55 @@ def test_particle_fluid_from_obj_with_writer(ctx, tmp_path):
                                sc.iterations, sc.dt, sc.sdf_spacing, 1, 1.0, steps, fp(xo), fp(vo)) == 0
         assert np.array_equal(xf, xo), k
     assert not os.path.exists(f"{out}frame_2.txt")
+
+
+def abi_elastoplastic(ctx, sc, x0, v0, frames, A, B, fracture):
+    """ParticleElastoplasticBody::advance composed from C-ABI calls."""
+    x, v = torch.from_numpy(x0.copy()).cuda(), torch.from_numpy(v0.copy()).cuda()
+    n, h, dt = x0.shape[0], sc.horizon, sc.dt
+    prm = pkhot.pbd_params(h, 0.005, 1000.0, 1, dt)
+    idx, el, tot = ctx.nq_build(x, h, sc.lo, sc.hi, 0)
+    ctx.pd_init(x, idx, el, 0, tot, h)
+    ones = torch.ones(n, device="cuda")
+    for _ in range(frames):
+        ctx.integrate(x, v, (0.0, -9.8, 0.0), dt)
+        idx, el, tot = ctx.nq_build(x, h, sc.lo, sc.hi, 0)
+        ctx.pd_begin(x, h, 0.05, 0.1, dt)
+        ctx.pd_compute_inverse_k(h)
+        for _ in range(10):
+            ctx.pd_enforce(x, h, 0.05, 0.1, dt)
+            ctx.pbd_solve(x, v, idx, el, 0, tot, prm)
+        ctx.pd_update_velocity(x, v, dt)
+        idx, el, tot = ctx.nq_build(x, h, sc.lo, sc.hi, 0)
+        if fracture:
+            ctx.pd_fracture(x, h, A, B, 0.05, 0.1)
+        else:
+            ctx.pd_rotate_rest_shape(x, h)
+            ctx.pd_set_bulk(ones)
+            ctx.pd_apply_yielding(x, h, A, B, 0.05, 0.1)
+            ctx.pd_reconstruct_rest_shape(x, idx, el, 0, tot, h, False)
+        ctx.viscosity(x, v, idx, el, 0, tot, 1.0, h, 5, dt)
+    ctx.check_status()
+    return x.cpu().numpy(), v.cpu().numpy()
+
+
+@pytest.mark.parametrize("fracture", [0, 1])
+def test_particle_elastoplastic_body_equals_module_calls(ctx, oracle, fracture):
+    sc = scenes.elastic_bar(seed=9, dims=(12, 6, 6), cap=0)
+    rng = np.random.default_rng(9)
+    x0 = (sc.x + rng.uniform(-0.02, 0.02, sc.x.shape) * sc.spacing).astype(np.float32)
+    v0 = rng.normal(0, 0.05, x0.shape).astype(np.float32)
+    v0[:, 0] += np.float32(0.5) * (x0[:, 1] - x0[:, 1].mean()) / np.float32(sc.spacing * 6)
+    n, steps = x0.shape[0], 3
+    L = fw()
+    f3 = ctypes.POINTER(ctypes.c_float)
+    L.pkf_elastoplastic_run.argtypes = [f3, f3, ctypes.c_int, f3, f3, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                        ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, f3, f3]
+    xo, vo = np.zeros_like(x0), np.zeros_like(x0)
+    c = 1e-3 if fracture else 1e-4
+    assert L.pkf_elastoplastic_run(fp(x0), fp(v0), n, fp(v3(sc.lo)), fp(v3(sc.hi)), sc.horizon, sc.dt, fracture,
+                                   c, 60.0, 0, steps, fp(xo), fp(vo)) == 0
+    A, B = oracle.drucker_prager(c, 60.0 / 180.0)
+    xa, va = abi_elastoplastic(ctx, sc, x0, v0, steps, A, B, fracture)
+    assert rel(xo, xa) < 1e-6
+    assert rel(vo, va) < 1e-5
