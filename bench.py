@@ -358,6 +358,70 @@ def measure_pd(local, steps, warmup, barrier):
             "step_roofline": {"bytes_per_particle_step": b, "frac": val * b / (peak * 1e9), "peak_source": kind}}
 
 
+EP_WORKLOAD = ("elastoplastic block 64x32x32 = 65,536 particles, spacing 0.004, horizon 3 spacing, dynamic "
+               "lists, cohesion 1e-4, friction angle 60, shear flow 0.5 m/s; ParticleElastoplasticBody frame: "
+               "integrate, query, 10 x (projection + 1-iteration DensityPBD), query, rest-shape rotation, "
+               "yielding, reconstruction, 5 viscosity sweeps, dt 1e-3")
+
+
+def measure_elastoplastic(local, steps, warmup, barrier):
+    """ParticleElastoplasticBody::advance (ParticleElastoplasticBody.cpp:73-91)
+    composed from C-ABI calls; device time per frame (the dynamic lists and the
+    reconstruction's bond count synchronise the host every frame, as the
+    reference's thrust::reduce does)."""
+    import torch
+    import pkhot
+
+    dev = torch.device("cuda", local)
+    sc = scenes.elastic_bar(seed=0, dims=(64, 32, 32), cap=0)
+    n, h, dt = sc.x.shape[0], sc.horizon, sc.dt
+    rng = np.random.default_rng(0)
+    x0 = (sc.x + rng.uniform(-0.02, 0.02, sc.x.shape) * sc.spacing).astype(np.float32)
+    v0 = np.zeros_like(x0)
+    v0[:, 0] = 0.5 * (x0[:, 1] - x0[:, 1].mean()) / (x0[:, 1].max() - x0[:, 1].mean())
+    ctx = pkhot.Context(local)
+    x, v = torch.from_numpy(x0).to(dev), torch.from_numpy(v0).to(dev)
+    prm = pkhot.pbd_params(h, 0.005, 1000.0, 1, dt)
+    A = float(np.float32(6.0 * 1e-4 * np.cos(60 / 180) / (3.0 + np.sin(60 / 180)) / np.sqrt(3.0)))
+    B = float(np.float32(2.0 * np.sin(60 / 180) / (3.0 + np.sin(60 / 180)) / np.sqrt(3.0)))
+    idx, el, tot = ctx.nq_build(x, h, sc.lo, sc.hi, 0)
+    ctx.pd_init(x, idx, el, 0, tot, h)
+    ones = torch.ones(n, device=dev)
+
+    def frame():
+        ctx.integrate(x, v, (0.0, -9.8, 0.0), dt)
+        i1, e1, t1 = ctx.nq_build(x, h, sc.lo, sc.hi, 0)
+        ctx.pd_begin(x, h, 0.05, 0.1, dt)
+        ctx.pd_compute_inverse_k(h)
+        for _ in range(10):
+            ctx.pd_enforce(x, h, 0.05, 0.1, dt)
+            ctx.pbd_solve(x, v, i1, e1, 0, t1, prm)
+        ctx.pd_update_velocity(x, v, dt)
+        i2, e2, t2 = ctx.nq_build(x, h, sc.lo, sc.hi, 0)
+        ctx.pd_rotate_rest_shape(x, h)
+        ctx.pd_set_bulk(ones)
+        ctx.pd_apply_yielding(x, h, A, B, 0.05, 0.1)
+        ctx.pd_reconstruct_rest_shape(x, i2, e2, 0, t2, h, False)
+        ctx.viscosity(x, v, i2, e2, 0, t2, 1.0, h, 5, dt)
+
+    for _ in range(warmup):
+        frame()
+    barrier()
+    e0, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.current_stream())
+    for _ in range(steps):
+        frame()
+    e1_.record(torch.cuda.current_stream())
+    barrier()
+    ctx.check_status()
+    ms = e0.elapsed_time(e1_) / steps
+    y1, y2, _ = ctx.pd_get_yield(n)
+    yielding = int((y2 > 0).sum())
+    ctx.close()
+    return {"workload": EP_WORKLOAD, "particles": n, "value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "steps": steps, "yielding_particles_last_frame": yielding}
+
+
 def measure_adjoint(local, fd_coords=16):
     """cfg4: float rollout with checkpoints, its reverse pass, and a check of
     the double-precision adjoint against central differences of double rollouts."""
@@ -589,6 +653,8 @@ def run_pk(args):
                                           max_over_ranks, rank, world)
     if not args.no_pd:
         line["peridynamics"] = measure_pd(local, max(3, min(args.steps, 20)), max(3, args.warmup), barrier)
+    if not args.no_pd:
+        line["elastoplastic"] = measure_elastoplastic(local, max(3, min(args.steps, 10)), 3, barrier)
     if not args.no_adjoint:
         line["adjoint"] = measure_adjoint(local)
     if rank == 0 and world == 1 and not args.no_cpu:
