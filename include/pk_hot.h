@@ -314,7 +314,9 @@ int pk_pd_apply_yielding(pk_ctx* ctx, const float* x, int n, const pk_plastic_pa
  * the current positions) as rest bonds placed by the inverse deformation
  * (PM_ComputeInverseDeformation :389-471, PM_ReconstructRestShape :309-371);
  * the others keep theirs.  The rest shape becomes a CSR list.  Synchronises
- * the stream (the new bond count sizes the list). */
+ * the stream (the new bond count sizes the list).  The reference raises the
+ * yield flag only through reconstruct_all, so without it a CSR rest shape is
+ * left as it is and the call returns at once. */
 int pk_pd_reconstruct_rest_shape(pk_ctx* ctx, const float* x, int n, const int* index, const int* elements,
                                  int cap, long long total, float horizon, int reconstruct_all,
                                  pk_stream stream);

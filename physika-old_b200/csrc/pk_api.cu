@@ -1052,6 +1052,14 @@ PK_API int pk_pd_reconstruct_rest_shape(pk_ctx* c, const float* x, int n, const 
     cudaSetDevice(c->device);
     if ((rc = ensure_plastic(c))) return rc;
     cudaStream_t st = (cudaStream_t)stream;
+    // The yield flag is only ever raised by reconstruct_all (PM_ComputeInvariants
+    // only clears it), so without it every particle keeps its bonds: once the
+    // rest shape is in CSR the reconstruction copies it unchanged, and it is
+    // skipped (no bond count to read back, no host synchronisation).
+    if (!reconstruct_all && c->pd_cap == 0) {
+        c->launches = 0;
+        return PK_OK;
+    }
     int l = 0;
     if (reconstruct_all) l += pk::pl_enable_all(c, st);
     l += pk::pl_recon_begin(c, x, index, cap, total, horizon, st);
