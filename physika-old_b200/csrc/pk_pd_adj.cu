@@ -93,7 +93,35 @@ struct PdBonds {
     const int* in_off;   // incoming bonds k->i of particle i: in_list[in_off[i] .. in_off[i+1])
     const int2* in_list; // (source k, bond slot)
     float h, mu, lambda;
+    float inv_h;         // 1/h: the kernels multiply where the reference divides
 };
+
+// CorrectedKernel Weight and WeightRR (Kernel.h:99-142) with q = r * (1/h).
+__device__ __forceinline__ float corr_w_f(float r, float inv_h)
+{
+    const float q = r * inv_h;
+    return q > 1.0f ? 0.0f : q * q * q * (1.0f - q * q);
+}
+__device__ __forceinline__ float corr_wrr_f(float r, float inv_h)
+{
+    const float q = r * inv_h;
+    return q > 1.0f ? 0.0f : q * (1.0f - q * q) * (inv_h * inv_h);
+}
+
+// unit_or_zero without the length: one reciprocal square root.
+template <class R>
+__device__ __forceinline__ void unit_fast(V3<R>& u)
+{
+    const R l2 = u.x * u.x + u.y * u.y + u.z * u.z;
+    if (l2 > (R)(kEpsilon * kEpsilon) && l2 > (R)1.4210854715202004e-14) {
+        const R is = rsqrt(l2);
+        u.x *= is;
+        u.y *= is;
+        u.z *= is;
+    } else {
+        u.x = u.y = u.z = (R)0;
+    }
+}
 
 // Every particle is handled by a group of kPdG lanes of one warp: lane `sub`
 // takes bonds sub, sub + kPdG, ... and the group's partial sums are combined
@@ -148,10 +176,12 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, int sub, R 
         const float e0 = B.rpos[3 * at] - ri0, e1 = B.rpos[3 * at + 1] - ri1, e2 = B.rpos[3 * at + 2] - ri2;
         const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
         if (r > kEpsilon) {
-            const float wt = corr_w(r, B.h);
+            const float wt = corr_w_f(r, B.inv_h);
             const V3<R> xj = ld3r<R>(x, j);
-            const R p[3] = {(xj.x - ci.x) / (R)B.h, (xj.y - ci.y) / (R)B.h, (xj.z - ci.z) / (R)B.h};
-            const R q[3] = {(R)(e0 / B.h * wt), (R)(e1 / B.h * wt), (R)(e2 / B.h * wt)};
+            const R ih = (R)B.inv_h;
+            const R p[3] = {(xj.x - ci.x) * ih, (xj.y - ci.y) * ih, (xj.z - ci.z) * ih};
+            const float qs = B.inv_h * wt;
+            const R q[3] = {(R)(e0 * qs), (R)(e1 * qs), (R)(e2 * qs)};
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) F[a][b] += p[a] * q[b];
             tw += wt;
@@ -224,7 +254,7 @@ __global__ void __launch_bounds__(kPdBlock) k_pd_W(PdBonds B, const RB* __restri
         const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
         const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
         if (!(r > 0.01f * B.h)) continue;
-        w += ml * (R)bulk[i] * (R)corr_wrr(r, B.h);
+        w += ml * (R)bulk[i] * (R)corr_wrr_f(r, B.inv_h);
     }
     for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
         const int2 kb = B.in_list[t];
@@ -235,7 +265,7 @@ __global__ void __launch_bounds__(kPdBlock) k_pd_W(PdBonds B, const RB* __restri
                     e2 = B.rpos[3 * k0 + 2] - B.rpos[3 * at + 2];
         const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
         if (!(r > 0.01f * B.h)) continue;
-        w += ml * (R)bulk[kb.x] * (R)corr_wrr(r, B.h);
+        w += ml * (R)bulk[kb.x] * (R)corr_wrr_f(r, B.inv_h);
     }
     w = gsum(w);
     if (L.valid && L.sub == 0) W[i] = w;
@@ -264,9 +294,9 @@ __global__ void __launch_bounds__(kPdBlock)
         const V3<R> xj = ld3(x, B.ridx[at]);
         V3<R> nf = mat_e(Fi, e0, e1, e2);
         V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
-        unit_or_zero(nf);
-        unit_or_zero(nc);
-        const R wrr = (R)corr_wrr(r, B.h), mu = (R)B.mu * bulk[i] * wrr, la = (R)B.lambda * bulk[i] * wrr;
+        unit_fast(nf);
+        unit_fast(nc);
+        const R wrr = (R)corr_wrr_f(r, B.inv_h), mu = (R)B.mu * bulk[i] * wrr, la = (R)B.lambda * bulk[i] * wrr;
         const R rr = (R)r;
         const V3<R> dj{xj.x - ci.x, xj.y - ci.y, xj.z - ci.z};
         acc.x += mu * (dj.x + rr * nf.x) + la * (dj.x + rr * nc.x);
@@ -286,9 +316,9 @@ __global__ void __launch_bounds__(kPdBlock)
         const V3<R> xk = ld3(x, k);
         V3<R> nf = mat_e(F + 9LL * k, e0, e1, e2);
         V3<R> nc{xk.x - ci.x, xk.y - ci.y, xk.z - ci.z};
-        unit_or_zero(nf);
-        unit_or_zero(nc);
-        const R wrr = (R)corr_wrr(r, B.h), mu = (R)B.mu * bulk[k] * wrr, la = (R)B.lambda * bulk[k] * wrr;
+        unit_fast(nf);
+        unit_fast(nc);
+        const R wrr = (R)corr_wrr_f(r, B.inv_h), mu = (R)B.mu * bulk[k] * wrr, la = (R)B.lambda * bulk[k] * wrr;
         const R rr = (R)r;
         const V3<R> dk{xk.x - ci.x, xk.y - ci.y, xk.z - ci.z};
         acc.x += mu * (dk.x - rr * nf.x) + la * (dk.x - rr * nc.x);
@@ -366,7 +396,7 @@ __global__ void __launch_bounds__(kPdBlock)
         V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
         const R lf = unit_or_zero(nf);
         unit_or_zero(nc);
-        const R wrr = (R)corr_wrr(r, B.h), rr = (R)r;
+        const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
         const R mu = (R)B.mu * bulk_i * wrr;
         const V3<R> da{ai.x - aj.x, ai.y - aj.y, ai.z - aj.z};
         // F path
@@ -432,8 +462,9 @@ __global__ void __launch_bounds__(kPdBlock)
         const float r = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
         // F_i depends on x_i through -(x_i)/h q_j for every first-loop bond
         if (r > kEpsilon) {
-            const float wt = corr_w(r, B.h);
-            const R q0 = (R)(f0 / B.h * wt), q1 = (R)(f1 / B.h * wt), q2 = (R)(f2 / B.h * wt);
+            const float wt = corr_w_f(r, B.inv_h);
+            const float qs = B.inv_h * wt;
+            const R q0 = (R)(f0 * qs), q1 = (R)(f1 * qs), q2 = (R)(f2 * qs);
             out.x -= Gi[0] * q0 + Gi[1] * q1 + Gi[2] * q2;
             out.y -= Gi[3] * q0 + Gi[4] * q1 + Gi[5] * q2;
             out.z -= Gi[6] * q0 + Gi[7] * q1 + Gi[8] * q2;
@@ -442,7 +473,7 @@ __global__ void __launch_bounds__(kPdBlock)
         const V3<R> xj = ld3r<R>(x, j), aj = ld3(a, j);
         V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
         const R lc = unit_or_zero(nc);
-        const R wrr = (R)corr_wrr(r, B.h), rr = (R)r;
+        const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
         const R la = (R)B.lambda * bulk_i * wrr, dw = ml * bulk_i * wrr;
         const V3<R> uc = unit_vjp(nc, lc, V3<R>{la * rr * (ai.x - aj.x), la * rr * (ai.y - aj.y), la * rr * (ai.z - aj.z)});
         out.x += dw * aj.x + uc.x;
@@ -460,9 +491,10 @@ __global__ void __launch_bounds__(kPdBlock)
                     f2 = B.rpos[3 * at + 2] - B.rpos[3 * k0 + 2];
         const float r = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
         if (r > kEpsilon) {
-            const float wt = corr_w(r, B.h);
+            const float wt = corr_w_f(r, B.inv_h);
             const R* Gk = G + 9LL * k;
-            const R q0 = (R)(f0 / B.h * wt), q1 = (R)(f1 / B.h * wt), q2 = (R)(f2 / B.h * wt);
+            const float qs = B.inv_h * wt;
+            const R q0 = (R)(f0 * qs), q1 = (R)(f1 * qs), q2 = (R)(f2 * qs);
             out.x += Gk[0] * q0 + Gk[1] * q1 + Gk[2] * q2;
             out.y += Gk[3] * q0 + Gk[4] * q1 + Gk[5] * q2;
             out.z += Gk[6] * q0 + Gk[7] * q1 + Gk[8] * q2;
@@ -471,7 +503,7 @@ __global__ void __launch_bounds__(kPdBlock)
         const V3<R> xk = ld3r<R>(x, k), ak = ld3(a, k);
         V3<R> nc{xk.x - ci.x, xk.y - ci.y, xk.z - ci.z};
         const R lc = unit_or_zero(nc);
-        const R wrr = (R)corr_wrr(r, B.h), rr = (R)r;
+        const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
         const R la = (R)B.lambda * (R)bulk[k] * wrr, dw = ml * (R)bulk[k] * wrr;
         const V3<R> uc = unit_vjp(nc, lc, V3<R>{la * rr * (ak.x - ai.x), la * rr * (ak.y - ai.y), la * rr * (ak.z - ai.z)});
         out.x += dw * ak.x - uc.x;
@@ -681,6 +713,7 @@ static PdBonds bonds_of(pk_ctx* c, float horizon, float mu, float lambda)
     B.h = horizon;
     B.mu = mu;
     B.lambda = lambda;
+    B.inv_h = 1.0f / horizon;
     return B;
 }
 
