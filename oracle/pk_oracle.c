@@ -509,6 +509,31 @@ void pko_plane_constrain(int n, float* x, const float origin[3], const float dir
     }
 }
 
+/* The polar rotation and the clamped inverse the plasticity restatement
+ * forms (pk_oracle_plastic.inc), for checking against the reference's
+ * compiled polarDecomposition (MatrixFunc.inl:81-98, svd3).  Row-major. */
+void pko_polar_rotation(const float* A9, float* R9)
+{
+    double A[3][3], R[3][3];
+    int a, b;
+    for (a = 0; a < 3; a++)
+        for (b = 0; b < 3; b++) A[a][b] = (double)A9[3 * a + b];
+    polar_rotation_f(A, R);
+    for (a = 0; a < 3; a++)
+        for (b = 0; b < 3; b++) R9[3 * a + b] = (float)R[a][b];
+}
+
+void pko_clamped_inverse(const float* M9, double thr, double fill, float* out9)
+{
+    float M[3][3], O[3][3];
+    int a, b;
+    for (a = 0; a < 3; a++)
+        for (b = 0; b < 3; b++) M[a][b] = M9[3 * a + b];
+    clamped_inverse_f(M, thr, fill, O);
+    for (a = 0; a < 3; a++)
+        for (b = 0; b < 3; b++) out9[3 * a + b] = O[a][b];
+}
+
 /* The float kernel functions the solver uses, for checking against the
  * reference's compiled SpikyKernel / SmoothKernel / CorrectedKernel. */
 void pko_kernels_f(int n, const float* r, float h, float* out5)

@@ -156,6 +156,12 @@ void pko_pd_fracture##sfx(int n, const real* x, const int* index, int cap, long 
 PKO_DECLARE(float, _f)
 PKO_DECLARE(double, _d)
 
+/* Polar rotation (row-major 3x3) and V D' U^T of a symmetric positive
+ * semi-definite matrix (D' = 1/D above thr, fill below): the quantities the
+ * plasticity restatement takes from polarDecomposition (MatrixFunc.inl:81-98). */
+void pko_polar_rotation(const float* A9, float* R9);
+void pko_clamped_inverse(const float* M9, double thr, double fill, float* out9);
+
 /* Threads used by the OpenMP loops (0 = library default). 1 = deterministic. */
 void pko_set_threads(int t);
 int  pko_max_threads(void);

@@ -42,6 +42,8 @@ def lib():
         L.pko_density_scaling.argtypes = [c_float, c_float, c_float,
                                           ctypes.POINTER(c_float), ctypes.POINTER(c_float)]
         L.pko_sdf_box_dims.argtypes = [_f32p, _f32p, c_float, _i32p]
+        L.pko_polar_rotation.argtypes = [_f32p, _f32p]
+        L.pko_clamped_inverse.argtypes = [_f32p, ctypes.c_double, ctypes.c_double, _f32p]
         for sfx, rp, rt in (("_f", _f32p, c_float), ("_d", _f64p, ctypes.c_double)):
             getattr(L, "pko_summation_density" + sfx).argtypes = [
                 c_int, rp, _i32p, _i32p, c_int, c_ll, rt, rt, rp]
@@ -421,3 +423,21 @@ def drucker_prager(c, phi):
     A = 6.0 * c * np.cos(phi) / (3.0 + np.sin(phi)) / np.sqrt(3.0)
     B = 2.0 * np.sin(phi) / (3.0 + np.sin(phi)) / np.sqrt(3.0)
     return float(np.float32(A)), float(np.float32(B))
+
+
+def polar_rotation(A):
+    """The polar rotation of each row-major 3x3 in A (n, 9)."""
+    A = np.ascontiguousarray(A, np.float32).reshape(-1, 9)
+    out = np.zeros_like(A)
+    for k in range(A.shape[0]):
+        lib().pko_polar_rotation(A[k], out[k])
+    return out
+
+
+def clamped_inverse(M, thr, fill=1.0):
+    """V D' U^T of each symmetric PSD row-major 3x3 in M (n, 9)."""
+    M = np.ascontiguousarray(M, np.float32).reshape(-1, 9)
+    out = np.zeros_like(M)
+    for k in range(M.shape[0]):
+        lib().pko_clamped_inverse(M[k], float(thr), float(fill), out[k])
+    return out
