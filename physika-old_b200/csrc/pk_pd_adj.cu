@@ -339,6 +339,99 @@ __global__ void __launch_bounds__(kPdBlock)
     xn[3 * i + 2] = ci.z + ((xo.z - ci.z) + acc.z) / den;
 }
 
+// The projection with each bond's term formed once.  A bond i->j's term in
+// D_j (the incoming sum above, seen from j) uses F_i, x_i, x_j and the rest
+// vector of i's shape, exactly like its term in D_i with the sign flipped:
+// mu (x_i - x_j - r n(F_i e)) + la (x_i - x_j - r n(x_i - x_j)) = -t_ij.  So
+// k_pd_FP computes F_i and every outgoing t_ij of particle i, keeps the sum
+// in own[i] and each t_ij in its bond slot (0 for a dead or too-short bond),
+// and k_pd_gather sums -t over the incoming slots: no neighbour F is
+// gathered and no bond is evaluated twice.
+template <class R>
+__global__ void __launch_bounds__(kPdBlock)
+    k_pd_FP(PdBonds B, const R* __restrict__ x, const R* __restrict__ bulk, R* __restrict__ Fout,
+            float* __restrict__ twout, R* __restrict__ own, R* __restrict__ tslot)
+{
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
+    R Fi[3][3];
+    float tw;
+    bool ident;
+    pd_deformation(B, x, i, L.sub, Fi, tw, ident);
+    if (L.valid && L.sub == 0) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) Fout[9LL * i + 3 * a + b] = Fi[a][b];
+        if (twout) twout[i] = ident ? -1.0f - tw : tw;
+    }
+    const long long a0 = pd_at(B.index, B.cap, i, 0);
+    const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
+    const V3<R> ci = ld3(x, i);
+    const int m = pd_size(B.index, B.cap, B.total, B.n, i);
+    V3<R> acc{0, 0, 0};
+    for (int e = L.sub; e < m; e += kPdG) {
+        const long long at = pd_at(B.index, B.cap, i, e);
+        V3<R> t{0, 0, 0};
+        const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
+        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        if (B.alive[at] && r > 0.01f * B.h) {
+            const V3<R> xj = ld3(x, B.ridx[at]);
+            V3<R> nf = V3<R>{Fi[0][0] * e0 + Fi[0][1] * e1 + Fi[0][2] * e2, Fi[1][0] * e0 + Fi[1][1] * e1 + Fi[1][2] * e2,
+                             Fi[2][0] * e0 + Fi[2][1] * e1 + Fi[2][2] * e2};
+            V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
+            unit_fast(nf);
+            unit_fast(nc);
+            const R wrr = (R)corr_wrr_f(r, B.inv_h), mu = (R)B.mu * bulk[i] * wrr, la = (R)B.lambda * bulk[i] * wrr;
+            const R rr = (R)r;
+            const V3<R> dj{xj.x - ci.x, xj.y - ci.y, xj.z - ci.z};
+            t = V3<R>{mu * (dj.x + rr * nf.x) + la * (dj.x + rr * nc.x), mu * (dj.y + rr * nf.y) + la * (dj.y + rr * nc.y),
+                      mu * (dj.z + rr * nf.z) + la * (dj.z + rr * nc.z)};
+            acc.x += t.x;
+            acc.y += t.y;
+            acc.z += t.z;
+        }
+        if (L.valid) {
+            R* o = tslot + 4 * at;
+            o[0] = t.x;
+            o[1] = t.y;
+            o[2] = t.z;
+        }
+    }
+    acc.x = gsum(acc.x);
+    acc.y = gsum(acc.y);
+    acc.z = gsum(acc.z);
+    if (L.valid && L.sub == 0) {
+        own[3 * i] = acc.x;
+        own[3 * i + 1] = acc.y;
+        own[3 * i + 2] = acc.z;
+    }
+}
+
+// xn = (xold + own - sum of the incoming bond terms) / (1 + W), written about x_i.
+template <class R>
+__global__ void __launch_bounds__(kPdBlock)
+    k_pd_gather(PdBonds B, const R* __restrict__ x, const R* __restrict__ xold, const R* __restrict__ own,
+                const R* __restrict__ tslot, const R* __restrict__ W, R* __restrict__ xn)
+{
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
+    V3<R> in{0, 0, 0};
+    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
+        const R* g = tslot + 4 * (long long)B.in_list[t].y;
+        in.x += g[0];
+        in.y += g[1];
+        in.z += g[2];
+    }
+    in.x = gsum(in.x);
+    in.y = gsum(in.y);
+    in.z = gsum(in.z);
+    if (!L.valid || L.sub != 0) return;
+    const V3<R> ci = ld3(x, i), oi = ld3(own, i), xo = ld3(xold, i);
+    const R den = (R)1 + W[i];
+    xn[3 * i] = ci.x + ((xo.x - ci.x) + (oi.x - in.x)) / den;
+    xn[3 * i + 1] = ci.y + ((xo.y - ci.y) + (oi.y - in.y)) / den;
+    xn[3 * i + 2] = ci.z + ((xo.z - ci.z) + (oi.z - in.z)) / den;
+}
+
 // ---- adjoint of one iteration
 
 // a = g/(1+W); xoldbar += a.
@@ -634,6 +727,9 @@ template <class R>
 struct PdWork {
     int cap_n = 0;
     R *F = nullptr, *W = nullptr, *xold = nullptr, *xa = nullptr, *vr = nullptr, *bulk = nullptr;
+    R* own = nullptr;       // 3 per particle: the sum of its outgoing bond terms
+    R* tslot = nullptr;     // 4 per bond slot: the bond's term
+    long long tslot_cap = 0;
     double *a = nullptr, *G = nullptr, *g = nullptr, *xoldbar = nullptr, *xb = nullptr,
            *vb = nullptr, *Wa = nullptr, *bulkbar = nullptr;
     // rollout record
@@ -676,7 +772,7 @@ static bool work_alloc(PdWork<R>& w, int n)
 {
     if (n <= w.cap_n) return true;
     const size_t m = (size_t)n;
-    bool ok = realloc_n(w.F, 9 * m) && realloc_n(w.W, m) && realloc_n(w.xold, 3 * m) &&
+    bool ok = realloc_n(w.F, 9 * m) && realloc_n(w.W, m) && realloc_n(w.xold, 3 * m) && realloc_n(w.own, 3 * m) &&
               realloc_n(w.xa, 3 * m) && realloc_n(w.vr, 3 * m) && realloc_n(w.bulk, m) &&
               realloc_n(w.a, 3 * m) && realloc_n(w.G, 9 * m) && realloc_n(w.g, 3 * m) &&
               realloc_n(w.xoldbar, 3 * m) && realloc_n(w.xb, 3 * m) && realloc_n(w.vb, 3 * m) &&
@@ -690,7 +786,7 @@ template <class R>
 static void work_free(PdWork<R>* w)
 {
     if (!w) return;
-    void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->a, w->G, w->g, w->xoldbar,
+    void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->own, w->tslot, w->a, w->G, w->g, w->xoldbar,
                   w->xb, w->vb, w->Wa, w->bulkbar, w->ckpt, w->seg, w->segF, w->segT};
     for (void* p : ps)
         if (p) cudaFree(p);
@@ -743,6 +839,7 @@ static PdWork<R>* ensure_work(pk_ctx* c, int n)
     PdWork<R>*& w = work_of<R>(c);
     if (!w) w = new PdWork<R>();
     if (!work_alloc(*w, n)) return nullptr;
+    if (!grow(w->tslot, w->tslot_cap, 4 * std::max(c->pd_total, 1LL))) return nullptr;
     return w;
 }
 
@@ -773,8 +870,8 @@ static int project(PdWork<R>& w, const PdBonds& B, R* x, const R* bulk, int iter
     R* cur = x;
     R* nxt = w.xa;
     for (int it = 0; it < iterations; ++it) {
-        k_pd_F<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.F, nullptr);
-        k_pd_P<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.xold, w.F, bulk, w.W, nxt);
+        k_pd_FP<R><<<nb128, kPdBlock, 0, st>>>(B, cur, bulk, w.F, nullptr, w.own, w.tslot);
+        k_pd_gather<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.xold, w.own, w.tslot, w.W, nxt);
         R* t = cur;
         cur = nxt;
         nxt = t;
@@ -818,8 +915,8 @@ int pd_enforce(pk_ctx* c, float* x, int n, float horizon, float mu, float lambda
     if (n <= 0) return 0;
     const PdBonds B = bonds_of(c, horizon, mu, lambda);
     const unsigned nb128 = pd_groups_blocks(n);
-    k_pd_F<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->F, nullptr);
-    k_pd_P<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->xold, w->F, c->pd_bulk, w->W, w->xa);
+    k_pd_FP<float><<<nb128, kPdBlock, 0, st>>>(B, x, c->pd_bulk, w->F, nullptr, w->own, w->tslot);
+    k_pd_gather<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->xold, w->own, w->tslot, w->W, w->xa);
     cudaMemcpyAsync(x, w->xa, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st);
     return 2;
 }
@@ -910,8 +1007,10 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
             for (int k = 0; k < iters; ++k) {
                 const long long slot = (long long)(s - s0) * iters + k;
                 R* Fk = w->segF + 9LL * n * slot;
-                k_pd_F<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, Fk, w->segT + 1LL * n * slot);
-                k_pd_P<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it, Fk, w->bulk, w->W, it + 3LL * n * (k + 1));
+                k_pd_FP<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, w->bulk, Fk, w->segT + 1LL * n * slot,
+                                                       w->own, w->tslot);
+                k_pd_gather<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it, w->own, w->tslot, w->W,
+                                                           it + 3LL * n * (k + 1));
             }
             k_pd_vel<R><<<nb3, 256, 0, st>>>(m3, vr, it + 3LL * n * iters, it, dt);
             cudaMemcpyAsync(xr, it + 3LL * n * iters, bytes, cudaMemcpyDeviceToDevice, st);
