@@ -612,6 +612,100 @@ __global__ void __launch_bounds__(kPdBlock)
     gout[3 * i + 2] = out.z;
 }
 
+// k_pd_adjC with each bond evaluated once.  The contribution of bond k->i to
+// dL/dx_i (the incoming loop above) is formed by the source k, which holds
+// G_k, x_k, a_k and the bond's rest vector: G_k q + dw a_k - u, u the
+// normalisation adjoint of n(x_k - x_i), the same u as in k's own term.
+// k_pd_adjC_push keeps k's own sum in gown[k] and the partner terms in the
+// bond slots; k_pd_adjC_gather adds the incoming slots.
+template <class R, class RX>
+__global__ void __launch_bounds__(kPdBlock)
+    k_pd_adjC_push(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ bulk, const R* __restrict__ a,
+                   const R* __restrict__ G, R* __restrict__ gown, R* __restrict__ slot)
+{
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
+    const long long a0 = pd_at(B.index, B.cap, i, 0);
+    const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
+    const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i);
+    const R bulk_i = (R)bulk[i];
+    const int m = pd_size(B.index, B.cap, B.total, B.n, i);
+    const R* Gi = G + 9LL * i;
+    const R ml = (R)B.mu + (R)B.lambda;
+    V3<R> out{0, 0, 0};
+    for (int e = L.sub; e < m; e += kPdG) {
+        const long long at = pd_at(B.index, B.cap, i, e);
+        V3<R> pt{0, 0, 0};  // the term for the bond's target
+        if (B.alive[at]) {
+            const int j = B.ridx[at];
+            const float f0 = B.rpos[3 * at] - ri0, f1 = B.rpos[3 * at + 1] - ri1, f2 = B.rpos[3 * at + 2] - ri2;
+            const float r = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
+            // F_i depends on x_i through -(x_i)/h q and on x_j through +(x_j)/h q
+            if (r > kEpsilon) {
+                const float wt = corr_w_f(r, B.inv_h);
+                const float qs = B.inv_h * wt;
+                const R q0 = (R)(f0 * qs), q1 = (R)(f1 * qs), q2 = (R)(f2 * qs);
+                const V3<R> gq{Gi[0] * q0 + Gi[1] * q1 + Gi[2] * q2, Gi[3] * q0 + Gi[4] * q1 + Gi[5] * q2,
+                               Gi[6] * q0 + Gi[7] * q1 + Gi[8] * q2};
+                out.x -= gq.x;
+                out.y -= gq.y;
+                out.z -= gq.z;
+                pt = gq;
+            }
+            if (r > 0.01f * B.h) {
+                const V3<R> xj = ld3r<R>(x, j), aj = ld3(a, j);
+                V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
+                const R lc = unit_or_zero(nc);
+                const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
+                const R la = (R)B.lambda * bulk_i * wrr, dw = ml * bulk_i * wrr;
+                const V3<R> uc =
+                    unit_vjp(nc, lc, V3<R>{la * rr * (ai.x - aj.x), la * rr * (ai.y - aj.y), la * rr * (ai.z - aj.z)});
+                out.x += dw * aj.x + uc.x;
+                out.y += dw * aj.y + uc.y;
+                out.z += dw * aj.z + uc.z;
+                pt.x += dw * ai.x - uc.x;
+                pt.y += dw * ai.y - uc.y;
+                pt.z += dw * ai.z - uc.z;
+            }
+        }
+        if (L.valid) {
+            R* o = slot + 4 * at;
+            o[0] = pt.x;
+            o[1] = pt.y;
+            o[2] = pt.z;
+        }
+    }
+    out.x = gsum(out.x);
+    out.y = gsum(out.y);
+    out.z = gsum(out.z);
+    if (!L.valid || L.sub != 0) return;
+    gown[3 * i] = out.x;
+    gown[3 * i + 1] = out.y;
+    gown[3 * i + 2] = out.z;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kPdBlock)
+    k_pd_adjC_gather(PdBonds B, const R* __restrict__ gown, const R* __restrict__ slot, R* __restrict__ gout)
+{
+    const PdLane L = pd_lane(B.n);
+    const int i = L.i;
+    V3<R> in{0, 0, 0};
+    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
+        const R* g = slot + 4 * (long long)B.in_list[t].y;
+        in.x += g[0];
+        in.y += g[1];
+        in.z += g[2];
+    }
+    in.x = gsum(in.x);
+    in.y = gsum(in.y);
+    in.z = gsum(in.z);
+    if (!L.valid || L.sub != 0) return;
+    gout[3 * i] = gown[3 * i] + in.x;
+    gout[3 * i + 1] = gown[3 * i + 1] + in.y;
+    gout[3 * i + 2] = gown[3 * i + 2] + in.z;
+}
+
 // ---- step pieces
 
 template <class R>
@@ -730,6 +824,9 @@ struct PdWork {
     R* own = nullptr;       // 3 per particle: the sum of its outgoing bond terms
     R* tslot = nullptr;     // 4 per bond slot: the bond's term
     long long tslot_cap = 0;
+    double* gown = nullptr;   // reverse pass: 3 per particle
+    double* aslot = nullptr;  // reverse pass: 4 per bond slot
+    long long aslot_cap = 0;
     double *a = nullptr, *G = nullptr, *g = nullptr, *xoldbar = nullptr, *xb = nullptr,
            *vb = nullptr, *Wa = nullptr, *bulkbar = nullptr;
     // rollout record
@@ -773,6 +870,7 @@ static bool work_alloc(PdWork<R>& w, int n)
     if (n <= w.cap_n) return true;
     const size_t m = (size_t)n;
     bool ok = realloc_n(w.F, 9 * m) && realloc_n(w.W, m) && realloc_n(w.xold, 3 * m) && realloc_n(w.own, 3 * m) &&
+              realloc_n(w.gown, 3 * m) &&
               realloc_n(w.xa, 3 * m) && realloc_n(w.vr, 3 * m) && realloc_n(w.bulk, m) &&
               realloc_n(w.a, 3 * m) && realloc_n(w.G, 9 * m) && realloc_n(w.g, 3 * m) &&
               realloc_n(w.xoldbar, 3 * m) && realloc_n(w.xb, 3 * m) && realloc_n(w.vb, 3 * m) &&
@@ -786,7 +884,8 @@ template <class R>
 static void work_free(PdWork<R>* w)
 {
     if (!w) return;
-    void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->own, w->tslot, w->a, w->G, w->g, w->xoldbar,
+    void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->own, w->tslot, w->gown, w->aslot, w->a, w->G,
+                  w->g, w->xoldbar,
                   w->xb, w->vb, w->Wa, w->bulkbar, w->ckpt, w->seg, w->segF, w->segT};
     for (void* p : ps)
         if (p) cudaFree(p);
@@ -840,6 +939,7 @@ static PdWork<R>* ensure_work(pk_ctx* c, int n)
     if (!w) w = new PdWork<R>();
     if (!work_alloc(*w, n)) return nullptr;
     if (!grow(w->tslot, w->tslot_cap, 4 * std::max(c->pd_total, 1LL))) return nullptr;
+    if (!grow(w->aslot, w->aslot_cap, 4 * std::max(c->pd_total, 1LL))) return nullptr;
     return w;
 }
 
@@ -1025,10 +1125,12 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
                 k_pd_adjB<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it + 3LL * n * (k + 1), w->bulk,
                                                              w->segF + 9LL * n * slot, w->segT + 1LL * n * slot,
                                                              w->a, w->G, w->bulkbar);
-                k_pd_adjC<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, w->bulk, w->a, w->G, w->g);
+                k_pd_adjC_push<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, w->bulk, w->a, w->G,
+                                                                      w->gown, w->aslot);
+                k_pd_adjC_gather<double><<<nb128, kPdBlock, 0, st>>>(B, w->gown, w->aslot, w->g);
             }
             k_pd_adj_tail<double><<<nb3, 256, 0, st>>>(m3, w->g, w->xoldbar, (double)dt, w->xb, w->vb);
-            l += 2 + 3 * iters;
+            l += 2 + 4 * iters;
         }
     }
     k_convert<R, double><<<nb3, 256, 0, st>>>(m3, w->xb, gx);
