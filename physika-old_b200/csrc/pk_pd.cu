@@ -100,17 +100,20 @@ __global__ void __launch_bounds__(256) k_fill_u8(unsigned char* __restrict__ p, 
 }
 
 // Stretch break (no reference counterpart): a bond dies for good once
-// |x_i - x_j| > (1 + s) * |rest_i - rest_j|.
+// |x_i - x_j| > (1 + s) * |rest_i - rest_j|.  kBreakG lanes per particle,
+// lane `sub` taking bonds sub, sub + kBreakG, ...
+constexpr int kBreakG = 8;
 __global__ void __launch_bounds__(256)
     k_pd_break(const float* __restrict__ x, int n, const int* __restrict__ index, int cap,
                long long total, const int* __restrict__ ridx, const float* __restrict__ rpos,
                unsigned char* __restrict__ alive, float s)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(gid / kBreakG), sub = (int)(gid % kBreakG);
     if (i >= n) return;
     long long a0 = pd_at(index, cap, i, 0);
     int m = pd_size(index, cap, total, n, i);
-    for (int e = 0; e < m; ++e) {
+    for (int e = sub; e < m; e += kBreakG) {
         long long at = pd_at(index, cap, i, e);
         if (!alive[at]) continue;
         int j = ridx[at];
@@ -155,7 +158,8 @@ int pd_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, floa
     if (n <= 0) return 0;
     int launches = 0;
     if (break_stretch > 0.f) {
-        k_pd_break<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, c->pd_index, c->pd_cap, c->pd_total,
+        k_pd_break<<<(unsigned)(((long long)n * kBreakG + 255) / 256), 256, 0, st>>>(x, n, c->pd_index, c->pd_cap,
+                                                                                      c->pd_total,
                                                                c->pd_rest_idx, c->pd_rest_pos, c->pd_alive,
                                                                break_stretch);
         ++launches;

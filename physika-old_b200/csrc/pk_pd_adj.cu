@@ -785,15 +785,41 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Each particle's incoming bonds in ascending bond slot (a fixed order).
-__global__ void __launch_bounds__(256) k_in_sort(int n, const int* __restrict__ off, int2* __restrict__ list)
+// Each particle's incoming bonds in ascending bond slot (a fixed order).  A
+// warp per particle: lists of up to 128 entries are held 4 per lane and each
+// entry goes to its rank (slots are distinct within a list); longer lists are
+// sorted by lane 0 in place.
+constexpr int kInSortWarps = 8;
+__global__ void __launch_bounds__(kInSortWarps * 32)
+    k_in_sort(int n, const int* __restrict__ off, int2* __restrict__ list)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    for (int a = off[i] + 1; a < off[i + 1]; ++a) {
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kInSortWarps + (threadIdx.x >> 5);
+    if (i >= n) return;  // the whole warp leaves together
+    const int o = off[i], m = off[i + 1] - o;
+    if (m <= 128) {
+        int2 v[4];
+        int rank[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = 32 * q + lane < m ? list[o + 32 * q + lane] : make_int2(0, 0x7fffffff);
+#pragma unroll
+        for (int sq = 0; sq < 4; ++sq)
+            for (int sl = 0; sl < 32; ++sl) {
+                const int w = __shfl_sync(0xffffffffu, v[sq].y, sl);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) rank[q] += w < v[q].y ? 1 : 0;
+            }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (32 * q + lane < m) list[o + rank[q]] = v[q];
+        return;
+    }
+    if (lane != 0) return;
+    for (int a = o + 1; a < o + m; ++a) {
         const int2 v = list[a];
         int b = a - 1;
-        while (b >= off[i] && list[b].y > v.y) {
+        while (b >= o && list[b].y > v.y) {
             list[b + 1] = list[b];
             --b;
         }
@@ -954,7 +980,8 @@ int pd_build_incoming(pk_ctx* c, cudaStream_t st)
     cudaMemsetAsync(c->pd_in_cnt, 0, sizeof(int) * (size_t)(n + 1), st);
     k_in_fill<<<nb, 256, 0, st>>>(n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_idx, c->pd_in_off,
                                   c->pd_in_cnt, c->pd_in);
-    k_in_sort<<<nb, 256, 0, st>>>(n, c->pd_in_off, c->pd_in);
+    k_in_sort<<<(unsigned)((n + kInSortWarps - 1) / kInSortWarps), kInSortWarps * 32, 0, st>>>(n, c->pd_in_off,
+                                                                                           c->pd_in);
     return 4 + scan_launches();
 }
 
