@@ -1,8 +1,9 @@
 // pk_plastic.cu -- ElastoplasticityModule and FractureModule
 // (Dynamics/ParticleSystem/ElastoplasticityModule.cu, FractureModule.cu) on
-// the context's peridynamics rest shape: one thread per particle walking its
-// own bonds, so every kernel updates only the bonds of its particle and the
-// rest shape can be rewritten in place.
+// the context's peridynamics rest shape.  Every kernel updates only the bonds
+// of its own particle, so the rest shape can be rewritten in place.  The
+// kernels with a double-precision eigen-decomposition per particle run one
+// thread per particle; the others split a particle's bonds over kPlG lanes.
 //
 // The reference's SVDs come from svd3_cuda.h (McAdams et al. 2011: U and V
 // rotations, the sign of det A on the smallest singular value).  What the
@@ -25,6 +26,39 @@ struct RestView {
 };
 
 __device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf((x * x + y * y) + z * z); }
+
+// kPlG lanes per particle: lane `sub` walks bonds sub, sub + kPlG, ...; the
+// group's partial sums are combined with xor shuffles in a fixed order.  The
+// idle lanes of the last group mirror particle n - 1 and write nothing.
+constexpr int kPlG = 8;
+constexpr int kPlBlock = 128;
+struct PlLane {
+    int i, sub;
+    bool valid;
+};
+__device__ __forceinline__ PlLane pl_lane(int n)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    PlLane L;
+    L.i = (int)(gid / kPlG);
+    L.sub = (int)(gid % kPlG);
+    L.valid = L.i < n;
+    if (!L.valid) L.i = n - 1;
+    return L;
+}
+__device__ __forceinline__ float gsum8(float v)
+{
+#pragma unroll
+    for (int o = kPlG / 2; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ void gsum8(float (&M)[3][3])
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) M[a][b] = gsum8(M[a][b]);
+}
 
 // Eigenpairs by decreasing eigenvalue.
 __device__ inline void eig_sorted(double A[3][3], double Q[3][3], double w[3])
@@ -131,7 +165,9 @@ __device__ inline float det3f(const float M[3][3])
            M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
 }
 
-// EM_RotateRestShape (ElastoplasticityModule.cu:568-644).
+// EM_RotateRestShape (ElastoplasticityModule.cu:568-644), one thread per
+// particle (the two double-precision eigen-decompositions dominate, and they
+// keep every lane of a warp busy this way).
 __global__ void __launch_bounds__(128) k_pl_rotate(RestView R, const float* __restrict__ x, float h)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -186,16 +222,18 @@ __global__ void __launch_bounds__(128) k_pl_rotate(RestView R, const float* __re
 }
 
 // I1 and the reference's J2 (PM_ComputeInvariants, ElastoplasticityModule.cu:43-128;
-// the J2 loop assigns, so only the last bond over 0.01 h counts).
-__device__ inline void invariants(const RestView& R, const float* __restrict__ x, float h, int i, float& I1,
-                                  float& J2)
+// the J2 loop assigns, so only the last bond over 0.01 h counts), by the
+// particle's lane group: the I1 sums are combined, and J2 is the term of the
+// group's largest qualifying bond index.
+__device__ inline void invariants(const RestView& R, const float* __restrict__ x, float h, int i, int sub,
+                                  float& I1, float& J2)
 {
     const long long a0 = pd_at(R.index, R.cap, i, 0);
     const float ri[3] = {R.rpos[3 * a0], R.rpos[3 * a0 + 1], R.rpos[3 * a0 + 2]};
     const int m = pd_size(R.index, R.cap, R.total, R.n, i);
     const double lim = 0.01 * (double)h;
-    float s1 = 0.f, tw = 0.f, j2 = 0.f;
-    for (int e = 1; e < m; ++e) {
+    float s1 = 0.f, tw = 0.f;
+    for (int e = 1 + sub; e < m; e += kPlG) {
         const long long at = pd_at(R.index, R.cap, i, e);
         const int j = R.ridx[at];
         const float* rj = R.rpos + 3 * at;
@@ -207,8 +245,12 @@ __device__ inline void invariants(const RestView& R, const float* __restrict__ x
             tw += wt;
         }
     }
+    s1 = gsum8(s1);
+    tw = gsum8(tw);
     s1 = tw > kEpsilon ? s1 / tw : 1.0f;
-    for (int e = 1; e < m; ++e) {
+    int last = -1;
+    float j2 = 0.f;
+    for (int e = 1 + sub; e < m; e += kPlG) {
         const long long at = pd_at(R.index, R.cap, i, e);
         const int j = R.ridx[at];
         const float* rj = R.rpos + 3 * at;
@@ -218,6 +260,16 @@ __device__ inline void invariants(const RestView& R, const float* __restrict__ x
             const float pl = len3(x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]);
             const float ratio = pl / r;
             j2 = (ratio - s1) * (ratio - s1) * wt;
+            last = e;
+        }
+    }
+#pragma unroll
+    for (int o = kPlG / 2; o >= 1; o >>= 1) {
+        const int ol = __shfl_xor_sync(0xffffffffu, last, o);
+        const float oj = __shfl_xor_sync(0xffffffffu, j2, o);
+        if (ol > last) {
+            last = ol;
+            j2 = oj;
         }
     }
     I1 = s1;
@@ -225,15 +277,16 @@ __device__ inline void invariants(const RestView& R, const float* __restrict__ x
 }
 
 // PM_ComputeInvariants: Drucker-Prager yield (a yielding particle keeps its flag).
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPlBlock)
     k_pl_invariants(RestView R, const float* __restrict__ x, const float* __restrict__ bulk, float h, float A,
                     float B, float mu, float lambda, float* __restrict__ y1, float* __restrict__ y2,
                     float* __restrict__ i1, unsigned char* __restrict__ byield)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R.n) return;
+    const PlLane L = pl_lane(R.n);
+    const int i = L.i;
     float I1, J2;
-    invariants(R, x, h, i, I1, J2);
+    invariants(R, x, h, i, L.sub, I1, J2);
+    if (!L.valid || L.sub != 0) return;
     const float sJ2 = J2 * mu * bulk[i];
     const float sD1 = (1.0f - I1) * lambda * bulk[i];
     const float lim = A + B * sD1;
@@ -266,16 +319,18 @@ __device__ inline void unit_or_zero3(float v[3])
 }
 
 // PM_ApplyYielding (ElastoplasticityModule.cu:165-226).
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPlBlock)
     k_pl_yield(RestView R, const float* __restrict__ x, const float* __restrict__ y1, const float* __restrict__ y2,
                const float* __restrict__ i1)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R.n) return;
+    const PlLane L = pl_lane(R.n);
+    const int i = L.i;
     const long long a0 = pd_at(R.index, R.cap, i, 0);
     const float ri[3] = {R.rpos[3 * a0], R.rpos[3 * a0 + 1], R.rpos[3 * a0 + 2]};
     const int m = pd_size(R.index, R.cap, R.total, R.n, i);
-    for (int e = 0; e < m; ++e) {
+    __syncwarp();  // every lane has read slot 0 before lane 0 of the group rewrites it
+    if (!L.valid) return;
+    for (int e = L.sub; e < m; e += kPlG) {
         const long long at = pd_at(R.index, R.cap, i, e);
         const int j = R.ridx[at];
         float* rj = R.rpos + 3 * at;
@@ -395,14 +450,15 @@ __global__ void __launch_bounds__(128)
 }
 
 // FractureModule's PM_ComputeInvariants (FractureModule.cu:15-105).
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPlBlock)
     k_pl_fracture(RestView R, const float* __restrict__ x, float* __restrict__ bulk, float h, float A, float B,
                   float mu, float lambda)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R.n) return;
+    const PlLane L = pl_lane(R.n);
+    const int i = L.i;
     float I1, J2;
-    invariants(R, x, h, i, I1, J2);
+    invariants(R, x, h, i, L.sub, I1, J2);
+    if (!L.valid || L.sub != 0) return;
     const float sJ2 = J2 * mu * bulk[i];
     const float sD1 = (1.0f - I1) * lambda * bulk[i];
     if (sJ2 > A + B * sD1) bulk[i] = 0.0f;
@@ -433,17 +489,19 @@ int pl_yield(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t
     const int n = c->pd_n;
     if (n <= 0) return 0;
     const RestView R = rest_view(c);
-    k_pl_invariants<<<blocks(n, 128), 128, 0, st>>>(R, x, c->pd_bulk, p->horizon, p->A, p->B, p->mu, p->lambda,
-                                                    c->pl_y1, c->pl_y2, c->pl_i1, c->pl_yield);
-    k_pl_yield<<<blocks(n, 128), 128, 0, st>>>(R, x, c->pl_y1, c->pl_y2, c->pl_i1);
+    const unsigned g = blocks((long long)n * kPlG, kPlBlock);
+    k_pl_invariants<<<g, kPlBlock, 0, st>>>(R, x, c->pd_bulk, p->horizon, p->A, p->B, p->mu, p->lambda, c->pl_y1,
+                                            c->pl_y2, c->pl_i1, c->pl_yield);
+    k_pl_yield<<<g, kPlBlock, 0, st>>>(R, x, c->pl_y1, c->pl_y2, c->pl_i1);
     return 2;
 }
 
 int pl_fracture(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t st)
 {
     if (c->pd_n <= 0) return 0;
-    k_pl_fracture<<<blocks(c->pd_n, 128), 128, 0, st>>>(rest_view(c), x, c->pd_bulk, p->horizon, p->A, p->B,
-                                                       p->mu, p->lambda);
+    k_pl_fracture<<<blocks((long long)c->pd_n * kPlG, kPlBlock), kPlBlock, 0, st>>>(rest_view(c), x, c->pd_bulk,
+                                                                                    p->horizon, p->A, p->B, p->mu,
+                                                                                    p->lambda);
     return 1;
 }
 
