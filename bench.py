@@ -553,9 +553,16 @@ def run_pk(args):
     ctx.nq_build(x, sc.radius, sc.lo, sc.hi, sc.cap, want_list=False)
     kbar, kunion, kmax = ctx.row_stats()
 
-    for _ in range(args.warmup):
+    # the context's autotuner picks the pass block size and the sweep's
+    # particles per pass in its first four frames (untimed); warm-up runs on
+    # until it has settled
+    ctx.autotune(True)
+    w = 0
+    while w < args.warmup or ctx.tuning()[2]:
         ctx.pbf_step(x, v, prm)
+        w += 1
     ctx.check_status()
+    tuned_pass, tuned_build, _ = ctx.tuning()
     launches_per_step = ctx.launch_count()
     barrier()
 
@@ -617,6 +624,7 @@ def run_pk(args):
                    "particles": n, "kbar": kbar, "solver_row_mean": kunion,
                    "solver_row_max": kmax, "iterations": sc.iterations,
                    "parallelism": "replicas" if world > 1 else "single",
+                   "tuned": {"pass_threads_per_block": tuned_pass, "build_particles_per_pass": tuned_build},
                    "l2": "working set > L2 (neighbour rows alone are > 1 GB); no flush"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,

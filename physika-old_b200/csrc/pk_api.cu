@@ -241,6 +241,8 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
 {
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
+    for (auto& e : c->tune.ev)
+        if (e) cudaEventDestroy(e);
     void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
                     c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau, c->tau_hint, c->pl_y1, c->pl_y2, c->pl_i1, c->pl_yield,
                     c->pl_invF, c->pl_sizes, c->pl_off, c->pl_rest_idx2, c->pl_rest_pos2,
@@ -286,6 +288,32 @@ PK_API int pk_ctx_status(pk_ctx* c, pk_stream stream)
 }
 
 PK_API int pk_last_launch_count(const pk_ctx* c) { return c ? c->launches : -1; }
+
+PK_API int pk_ctx_autotune(pk_ctx* c, int enable)
+{
+    if (!c) return PK_ERR_ARG;
+    cudaSetDevice(c->device);
+    auto& t = c->tune;
+    t = pk_ctx::Tune{t.on, 0, t.pass_block, t.build_pb, {0, 0, 0}, {0, 0, 0}, {t.ev[0], t.ev[1], t.ev[2], t.ev[3]}};
+    if (!enable) {
+        t.on = false;
+        return PK_OK;
+    }
+    for (auto& e : t.ev)
+        if (!e && cudaEventCreate(&e) != cudaSuccess) return fail(c, PK_ERR_CUDA, "cudaEventCreate failed");
+    t.on = true;
+    t.frame = 0;
+    return PK_OK;
+}
+
+PK_API int pk_ctx_tuning(const pk_ctx* c, int* pass_block, int* build_particles, int* active)
+{
+    if (!c) return PK_ERR_ARG;
+    if (pass_block) *pass_block = c->tune.pass_block;
+    if (build_particles) *build_particles = c->tune.build_pb;
+    if (active) *active = c->tune.on ? 1 : 0;
+    return PK_OK;
+}
 
 PK_API int pk_ctx_profile(pk_ctx* c, int enable)
 {
@@ -658,6 +686,37 @@ namespace {
 
 // One frame for one scene, or for several scenes concatenated in caller order
 // (scene_off: device offsets, nscenes + 1 entries) that share the parameters.
+// Reads the trial frame's build and solve times (this synchronises the
+// stream) and, after the last trial, keeps the fastest shapes.
+void tune_record(pk_ctx* c, int trial)
+{
+    auto& t = c->tune;
+    float build = 0.f, solve = 0.f;
+    if (cudaEventSynchronize(t.ev[3]) != cudaSuccess || cudaEventElapsedTime(&build, t.ev[0], t.ev[1]) != cudaSuccess ||
+        cudaEventElapsedTime(&solve, t.ev[2], t.ev[3]) != cudaSuccess) {
+        cudaGetLastError();
+        t.on = false;
+        t.pass_block = 256;
+        t.build_pb = 16;
+        return;
+    }
+    const int pi = t.pass_block == 128 ? 0 : (t.pass_block == 512 ? 2 : 1);
+    const int bi = t.build_pb == 8 ? 1 : (t.build_pb == 12 ? 2 : 0);
+    if (t.pass_ms[pi] == 0.f || solve < t.pass_ms[pi]) t.pass_ms[pi] = solve;
+    if (t.build_ms[bi] == 0.f || build < t.build_ms[bi]) t.build_ms[bi] = build;
+    t.frame = trial + 1;
+    if (t.frame < 4) return;
+    int best = 1;
+    for (int k = 0; k < 3; ++k)
+        if (t.pass_ms[k] < t.pass_ms[best]) best = k;
+    t.pass_block = best == 0 ? 128 : (best == 2 ? 512 : 256);
+    int bb = 0;
+    for (int k = 1; k < 3; ++k)
+        if (t.build_ms[k] < t.build_ms[bb]) bb = k;
+    t.build_pb = bb == 1 ? 8 : (bb == 2 ? 12 : 16);
+    t.on = false;
+}
+
 int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, float* rho_out,
                   const int* scene_off, int nscenes, pk_stream stream, const char* what)
 {
@@ -685,6 +744,14 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
         return rc;
     pk::SdfView sv{};
     if (p->boundary) sv = pk::sdf_view(c);
+    // autotuning: this frame's trial shapes (4 frames: pass blocks 128, 256,
+    // 512 and build passes of 8, 12 and 16 particles)
+    static const int kTrialPass[4] = {128, 256, 512, 256}, kTrialBuild[4] = {16, 8, 12, 16};
+    const int trial = c->tune.on ? c->tune.frame : -1;
+    if (trial >= 0) {
+        c->tune.pass_block = kTrialPass[trial];
+        c->tune.build_pb = kTrialBuild[trial];
+    }
     // The build state is recorded before anything is launched: the solver
     // passes read the row stride from the context.
     c->nq_valid = false;
@@ -707,6 +774,7 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     c->launches = l;
     if ((rc = check_launch(c, what))) return rc;
     c->nq_valid = true;  // for batched scenes: the union of the scenes' lists
+    if (trial >= 0) tune_record(c, trial);
     return PK_OK;
 }
 

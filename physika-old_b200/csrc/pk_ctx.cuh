@@ -110,6 +110,18 @@ struct pk_ctx {
     float* pl_rest_pos2 = nullptr;
     long long pl_cap_rest2 = 0;
     bool pd_begun = false;          // pk_pd_begin has run since pk_pd_init
+    // Autotuner of the frame kernels (pk_ctx_autotune): a few trial frames
+    // time the pass block sizes and the build's particles per pass; the
+    // choices change no result.
+    struct Tune {
+        bool on = false;
+        int frame = 0;
+        int pass_block = 256;   // Jacobi pass threads per block: 128, 256, 512
+        int build_pb = 16;      // k_build particles per pass: 8, 12 or 16
+        float pass_ms[3] = {0, 0, 0};
+        float build_ms[3] = {0, 0, 0};
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // build start/end, solve start/end
+    } tune;
     int* pd_in_cnt = nullptr;   // incoming bonds per particle (n + 1)
     int* pd_in_off = nullptr;   // their CSR offsets (n + 1)
     int2* pd_in = nullptr;      // (source particle, bond slot) of every incoming bond

@@ -83,7 +83,8 @@ struct BuildArgs {
     int* err;
 };
 
-// Particles of one pass, held in registers by every lane.
+// Particles of one pass, held in registers by every lane: 16, or 8 or 12 when
+// the context's autotuner measured that faster (the hit rows are the same).
 constexpr int kPB = 16;
 
 // Per-warp shared state of the sweep: the 27 neighbour ranges as (begin,
@@ -113,17 +114,17 @@ __device__ __forceinline__ float4 fetch_cand(const float4* __restrict__ xs, cons
 // One pass of the sweep: kPB particles in registers against every candidate
 // chunk.  kChecked guards the row bound; a cell whose 27 ranges hold at most
 // row_cap candidates cannot overflow a row and runs unchecked.
-template <bool kChecked>
+template <bool kChecked, int KPB>
 __device__ __forceinline__ void sweep(const BuildArgs& A, const SweepSmem& S, int total, int p0, int m,
-                                      const float (&px)[kPB], const float (&py)[kPB], const float (&pz)[kPB],
-                                      int (&cnt)[kPB], int lane, unsigned lt)
+                                      const float (&px)[KPB], const float (&py)[KPB], const float (&pz)[KPB],
+                                      int (&cnt)[KPB], int lane, unsigned lt)
 {
     uint2* const row0 = A.hits + (long long)p0 * A.row_cap;
     for (int c0 = 0; c0 < total; c0 += 32) {
         int t;
         const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
 #pragma unroll
-        for (int p = 0; p < kPB; ++p) {
+        for (int p = 0; p < KPB; ++p) {
             if (p >= m) break;  // warp-uniform
             const float d2 = exact_d2(make_float4(px[p], py[p], pz[p], 0.f), cx);
             const bool hit = d2 < A.T;
@@ -144,6 +145,7 @@ __device__ __forceinline__ void sweep(const BuildArgs& A, const SweepSmem& S, in
 #ifndef PK_BUILD_MIN_BLOCKS
 #define PK_BUILD_MIN_BLOCKS 1  // resident blocks per SM asked of the register allocator
 #endif
+template <int KPB>
 __global__ void __launch_bounds__(kBuildWarps * 32, PK_BUILD_MIN_BLOCKS) k_build(BuildArgs A)
 {
     extern __shared__ int smem_i[];
@@ -179,12 +181,12 @@ __global__ void __launch_bounds__(kBuildWarps * 32, PK_BUILD_MIN_BLOCKS) k_build
         const int total = __shfl_sync(kFull, incl, 31);
         if (lane == 31) S.roff[32] = total;
         __syncwarp();
-        for (int p0 = rng.x; p0 < rng.y; p0 += kPB) {
-            const int m = min(kPB, rng.y - p0);
-            float px[kPB], py[kPB], pz[kPB];
-            int cnt[kPB];
+        for (int p0 = rng.x; p0 < rng.y; p0 += KPB) {
+            const int m = min(KPB, rng.y - p0);
+            float px[KPB], py[KPB], pz[KPB];
+            int cnt[KPB];
 #pragma unroll
-            for (int p = 0; p < kPB; ++p) {
+            for (int p = 0; p < KPB; ++p) {
                 if (p < m) {
                     const float4 q = __ldg(A.xs + p0 + p);
                     px[p] = q.x;
@@ -196,11 +198,11 @@ __global__ void __launch_bounds__(kBuildWarps * 32, PK_BUILD_MIN_BLOCKS) k_build
                 cnt[p] = 0;
             }
             if (total <= A.row_cap)
-                sweep<false>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
+                sweep<false, KPB>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
             else
-                sweep<true>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
+                sweep<true, KPB>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
 #pragma unroll
-            for (int p = 0; p < kPB; ++p) {
+            for (int p = 0; p < KPB; ++p) {
                 if (lane == p && p < m) {
                     const int s = p0 + p;
                     A.hcnt[s] = min(cnt[p], A.row_cap);
@@ -586,7 +588,13 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // a persistent grid: as many warps per SM as registers and shared memory allow
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build, kBuildWarps * 32, kBuildSmem);
+    const int pbn = c->tune.build_pb;
+    if (pbn == 8)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<8>, kBuildWarps * 32, kBuildSmem);
+    else if (pbn == 12)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<12>, kBuildWarps * 32, kBuildSmem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<kPB>, kBuildWarps * 32, kBuildSmem);
     if (sms <= 0) sms = 148;
     if (per_sm <= 0) per_sm = 1;
     int launches = 0;
@@ -608,7 +616,14 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     A.err = c->d_err;
     const int blocks = std::min((n + kBuildWarps - 1) / kBuildWarps, sms * per_sm);
     prof_begin(c, PK_PROF_SELECT, st);
-    k_build<<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
+    if (c->tune.on) cudaEventRecord(c->tune.ev[0], st);
+    if (pbn == 8)
+        k_build<8><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
+    else if (pbn == 12)
+        k_build<12><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
+    else
+        k_build<kPB><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
+    if (c->tune.on) cudaEventRecord(c->tune.ev[1], st);
     ++launches;
     if (capped) {
         const int sb = (int)std::min<long long>(((long long)n + 32 * kSelWarps - 1) / (32 * kSelWarps), (long long)sms * 8);

@@ -199,7 +199,8 @@ __device__ __forceinline__ void dens_one(const float4& a, const float4& xi, cons
     s.sg.x = fmaf(w, w, s.sg.x);
 }
 
-__global__ void __launch_bounds__(kPassBlock, PK_PASS_MINB)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
     k_pass_density2(const float4* __restrict__ xs, const int* __restrict__ rows,
                     const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
                     float4* __restrict__ xl, float* __restrict__ rho_out)
@@ -267,7 +268,8 @@ __device__ __forceinline__ void disp_one(const float4& a, int v, const float4& x
     s.az.x = fmaf(c, dz, s.az.x);
 }
 
-__global__ void __launch_bounds__(kPassBlock, PK_PASS_MINB)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
     k_pass_disp2(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
                  int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
 {
@@ -342,7 +344,8 @@ __global__ void __launch_bounds__(256)
 // One K_ApplyViscosity sweep over N(i) (the rows' first |N(i)| entries):
 // v_i = v_old,i/(1+b) + (sum w v_j / sum w) b/(1+b); b = 0 and sum w = 1 when
 // sum w < EPSILON.
-__global__ void __launch_bounds__(256)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
     k_pass_visc(const float4* __restrict__ xs, const float4* __restrict__ vin, const float4* __restrict__ vold,
                 const int* __restrict__ rows, const int2* __restrict__ rcnt, int row_cap, int n, ViscK k_,
                 float4* __restrict__ vout)
@@ -417,11 +420,51 @@ __global__ void __launch_bounds__(256)
     vs[s] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f);
 }
 
+// The Jacobi passes at the block size the context's autotuner chose (128,
+// 256 or 512 threads; one thread per particle, so the results do not depend
+// on it).
+template <template <int> class Launch, class... Args>
+static void by_block(int block, Args&&... args)
+{
+    if (block == 128)
+        Launch<128>::run(args...);
+    else if (block == 512)
+        Launch<512>::run(args...);
+    else
+        Launch<256>::run(args...);
+}
+template <int B>
+struct LaunchDensity {
+    static void run(unsigned nb, cudaStream_t st, const float4* cur, const int* rows, const int2* rcnt, int row_cap,
+                    int n, PassK pk, float4* xl, float* rho)
+    {
+        k_pass_density2<B><<<nb, B, 0, st>>>(cur, rows, rcnt, row_cap, n, pk, xl, rho);
+    }
+};
+template <int B>
+struct LaunchDisp {
+    static void run(unsigned nb, cudaStream_t st, const float4* xl, const int* rows, const int2* rcnt, int row_cap,
+                    int n, PassK pk, float4* out)
+    {
+        k_pass_disp2<B><<<nb, B, 0, st>>>(xl, rows, rcnt, row_cap, n, pk, out);
+    }
+};
+template <int B>
+struct LaunchVisc {
+    static void run(unsigned nb, cudaStream_t st, const float4* xs, const float4* vin, const float4* vold,
+                    const int* rows, const int2* rcnt, int row_cap, int n, ViscK vk, float4* vout)
+    {
+        k_pass_visc<B><<<nb, B, 0, st>>>(xs, vin, vold, rows, rcnt, row_cap, n, vk, vout);
+    }
+};
+
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
                    float* x, float* v, float* rho_out, cudaStream_t st, float viscosity, int vis_iterations)
 {
     if (n <= 0) return 0;
-    const unsigned nb1 = (unsigned)((n + 255) / 256), nbp = (unsigned)((n + kPassBlock - 1) / kPassBlock);
+    const int pb = c->tune.pass_block;
+    const unsigned nb1 = (unsigned)((n + 255) / 256), nbp = (unsigned)((n + pb - 1) / pb);
+    if (c->tune.on) cudaEventRecord(c->tune.ev[2], st);
     int launches = 0;
     const float4* cur = c->xs0;
     const PassK pk = pass_k(k, mass);
@@ -431,17 +474,18 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
         if (PK_PASS_F32X2)
-            k_pass_density2<<<nbp, kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
-                                                        last ? c->rho : nullptr);
+            by_block<LaunchDensity>(pb, nbp, st, cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                    last ? c->rho : nullptr);
         else
-            k_pass_density<<<nbp, kPassBlock, 0, st>>>(cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
-                                                       last ? c->rho : nullptr);
+            k_pass_density<<<(n + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(
+                cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb, last ? c->rho : nullptr);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
         if (PK_PASS_F32X2)
-            k_pass_disp2<<<nbp, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+            by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
         else
-            k_pass_disp<<<nbp, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+            k_pass_disp<<<(n + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt,
+                                                                                 c->row_cap, n, pk, c->xa);
         prof_end(c, PK_PROF_DISP, st);
         cur = c->xa;
         launches += 2;
@@ -456,7 +500,7 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
         float4* vin = c->vv;
         float4* vout = c->xb;
         for (int t = 0; t < vis_iterations; ++t) {
-            k_pass_visc<<<nbp, kPassBlock, 0, st>>>(cur, vin, c->vs, c->rows, c->rcnt, c->row_cap, n, vk, vout);
+            by_block<LaunchVisc>(pb, nbp, st, cur, vin, c->vs, c->rows, c->rcnt, c->row_cap, n, vk, vout);
             float4* tmp = vin;
             vin = vout;
             vout = tmp;
@@ -468,6 +512,7 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
         ++launches;
     }
     prof_end(c, PK_PROF_FINISH, st);
+    if (c->tune.on) cudaEventRecord(c->tune.ev[3], st);
     return launches;
 }
 

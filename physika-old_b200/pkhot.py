@@ -15,7 +15,7 @@ PK_OK, PK_ERR_ARG, PK_ERR_CUDA, PK_ERR_CAPACITY, PK_ERR_STATE, PK_ERR_NOMEM = ra
 
 EXPORTED = [
     "pk_ctx_create", "pk_ctx_destroy", "pk_last_error", "pk_ctx_status", "pk_last_launch_count",
-    "pk_ctx_profile", "pk_ctx_profile_read",
+    "pk_ctx_profile", "pk_ctx_profile_read", "pk_ctx_autotune", "pk_ctx_tuning",
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
     "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain", "pk_viscosity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
@@ -102,6 +102,8 @@ def load():
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
         "pk_pd_get_rest_shape": ([P, P, P, P, P], I),
+        "pk_ctx_autotune": ([P, I], I),
+        "pk_ctx_tuning": ([P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "pk_pd_compute_inverse_k": ([P, F, P], I),
         "pk_pd_begin": ([P, P, I, ctypes.POINTER(PdParams), P], I),
         "pk_pd_enforce": ([P, P, I, ctypes.POINTER(PdParams), P], I),
@@ -351,6 +353,16 @@ class Context:
         fn = self.L.pk_pd_rollout_backward_f64 if xbar.dtype == torch.float64 else self.L.pk_pd_rollout_backward
         self._check(fn(self.h, _ptr(xbar), _ptr(vbar), _ptr(gx), _ptr(gv), _ptr(gb), _stream()))
         return gx, gv, gb
+
+    # ---- autotuning of the frame kernels
+    def autotune(self, enable=True):
+        self._check(self.L.pk_ctx_autotune(self.h, int(bool(enable))))
+
+    def tuning(self):
+        """(pass threads per block, build particles per pass, trials remaining?)."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.pk_ctx_tuning(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, bool(c.value)
 
     # ---- ElasticityModule step by step, ElastoplasticityModule, FractureModule
     def pd_compute_inverse_k(self, horizon):
