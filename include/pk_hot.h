@@ -228,7 +228,7 @@ int pk_last_launch_count(const pk_ctx* ctx);
 /* Autotuning of the frame kernels (no reference counterpart).  With enable,
  * the next four pk_pbf_step / pk_pbf_step_batched calls are trial frames: they
  * run the Jacobi passes at 128, 256 and 512 threads per block and the
- * neighbour sweep with 8, 12 and 16 particles per pass, time them (each trial
+ * neighbour sweep with 4, 8 and 16 particles per pass, time them (each trial
  * frame synchronises its stream, so do not capture them in a graph), and keep
  * the fastest shapes for the context.  The shapes change no result.
  * pk_ctx_tuning reports the shapes in use and whether trials remain. */

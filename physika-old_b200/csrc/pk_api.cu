@@ -697,11 +697,11 @@ void tune_record(pk_ctx* c, int trial)
         cudaGetLastError();
         t.on = false;
         t.pass_block = 256;
-        t.build_pb = 16;
+        t.build_pb = 8;
         return;
     }
     const int pi = t.pass_block == 128 ? 0 : (t.pass_block == 512 ? 2 : 1);
-    const int bi = t.build_pb == 8 ? 1 : (t.build_pb == 12 ? 2 : 0);
+    const int bi = t.build_pb == 8 ? 1 : (t.build_pb == 4 ? 2 : 0);
     if (t.pass_ms[pi] == 0.f || solve < t.pass_ms[pi]) t.pass_ms[pi] = solve;
     if (t.build_ms[bi] == 0.f || build < t.build_ms[bi]) t.build_ms[bi] = build;
     t.frame = trial + 1;
@@ -713,7 +713,7 @@ void tune_record(pk_ctx* c, int trial)
     int bb = 0;
     for (int k = 1; k < 3; ++k)
         if (t.build_ms[k] < t.build_ms[bb]) bb = k;
-    t.build_pb = bb == 1 ? 8 : (bb == 2 ? 12 : 16);
+    t.build_pb = bb == 1 ? 8 : (bb == 2 ? 4 : 16);
     t.on = false;
 }
 
@@ -745,8 +745,8 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     pk::SdfView sv{};
     if (p->boundary) sv = pk::sdf_view(c);
     // autotuning: this frame's trial shapes (4 frames: pass blocks 128, 256,
-    // 512 and build passes of 8, 12 and 16 particles)
-    static const int kTrialPass[4] = {128, 256, 512, 256}, kTrialBuild[4] = {16, 8, 12, 16};
+    // 512 and build passes of 4, 8 and 16 particles)
+    static const int kTrialPass[4] = {128, 256, 512, 256}, kTrialBuild[4] = {16, 8, 4, 16};
     const int trial = c->tune.on ? c->tune.frame : -1;
     if (trial >= 0) {
         c->tune.pass_block = kTrialPass[trial];

@@ -117,7 +117,7 @@ struct pk_ctx {
         bool on = false;
         int frame = 0;
         int pass_block = 256;   // Jacobi pass threads per block: 128, 256, 512
-        int build_pb = 16;      // k_build particles per pass: 8, 12 or 16
+        int build_pb = 8;       // k_build particles per pass: 4, 8 or 16 (8 measured fastest at 2M)
         float pass_ms[3] = {0, 0, 0};
         float build_ms[3] = {0, 0, 0};
         cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // build start/end, solve start/end

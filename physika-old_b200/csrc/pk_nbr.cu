@@ -9,10 +9,11 @@
 // row holds N(i) plus {j : i in N(j)} with two flag bits, so a pair's
 // multiplicity in i's displacement is known without atomics.
 //
-//   k_build (one warp per occupied cell, passes of up to 16 particles): every
-//     lane holds the pass's particles in registers and takes one candidate of
-//     each 32-wide chunk of the 27 neighbour ranges (a coalesced load), so a
-//     lane runs 16 independent pair tests per chunk; one ballot per particle
+//   k_build (one warp per occupied cell, passes of up to 8 particles, 4 or 16
+//     when the context's autotuner measured that faster): every lane holds the
+//     pass's particles in registers and takes one candidate of each 32-wide
+//     chunk of the 27 neighbour ranges (a coalesced load), so a lane runs up to
+//     8 independent pair tests per chunk; one ballot per particle
 //     appends the chunk's hits (sorted index, d2) to its hit row in candidate
 //     order.  The hit test compares the rounded squared distance with the
 //     precomputed float T (sqrt_rn(d2) < h  <=>  d2 < T, sqrt_rn being
@@ -83,8 +84,9 @@ struct BuildArgs {
     int* err;
 };
 
-// Particles of one pass, held in registers by every lane: 16, or 8 or 12 when
-// the context's autotuner measured that faster (the hit rows are the same).
+// Particles of one pass, held in registers by every lane: 8 by default, 4 or
+// 16 when the context's autotuner measured that faster (the hit rows are the
+// same).
 constexpr int kPB = 16;
 
 // Per-warp shared state of the sweep: the 27 neighbour ranges as (begin,
@@ -591,8 +593,8 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     const int pbn = c->tune.build_pb;
     if (pbn == 8)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<8>, kBuildWarps * 32, kBuildSmem);
-    else if (pbn == 12)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<12>, kBuildWarps * 32, kBuildSmem);
+    else if (pbn == 4)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<4>, kBuildWarps * 32, kBuildSmem);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build<kPB>, kBuildWarps * 32, kBuildSmem);
     if (sms <= 0) sms = 148;
@@ -619,8 +621,8 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     if (c->tune.on) cudaEventRecord(c->tune.ev[0], st);
     if (pbn == 8)
         k_build<8><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
-    else if (pbn == 12)
-        k_build<12><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
+    else if (pbn == 4)
+        k_build<4><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
     else
         k_build<kPB><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
     if (c->tune.on) cudaEventRecord(c->tune.ev[1], st);

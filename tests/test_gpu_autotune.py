@@ -1,6 +1,6 @@
 """The frame autotuner (pk_ctx_autotune): its four trial frames run the
-Jacobi passes at 128/256/512 threads per block and the neighbour sweep with 8,
-12 and 16 particles per pass.  Those shapes change no result, so a tuned context
+Jacobi passes at 128/256/512 threads per block and the neighbour sweep with 4,
+8 and 16 particles per pass.  Those shapes change no result, so a tuned context
 must step bit for bit like an untuned one, and it must settle on one of the
 trial shapes."""
 import numpy as np
@@ -35,9 +35,9 @@ def test_autotuned_frames_equal_untuned(viscosity):
         ctx.check_status()
         pb, bp, active = ctx.tuning()
         if tune:
-            assert not active and pb in (128, 256, 512) and bp in (8, 12, 16)
+            assert not active and pb in (128, 256, 512) and bp in (4, 8, 16)
         else:
-            assert (pb, bp, active) == (256, 16, False)
+            assert (pb, bp, active) == (256, 8, False)
         out.append((x.cpu().numpy(), v.cpu().numpy()))
         ctx.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
