@@ -556,7 +556,7 @@ def run_pk(args):
     # the context's autotuner picks the pass block size and the sweep's
     # particles per pass in its first four frames (untimed); warm-up runs on
     # until it has settled
-    ctx.autotune(True)
+    ctx.autotune(not args.no_autotune)
     w = 0
     while w < args.warmup or ctx.tuning()[2]:
         ctx.pbf_step(x, v, prm)
@@ -688,6 +688,10 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes comparison")
     ap.add_argument("--no-pd", action="store_true", help="skip the peridynamics bar")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable rollout")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default shapes (256 threads per pass block, 8 particles per sweep pass) "
+                         "instead of tuning during warm-up; for profiler captures, whose serialised "
+                         "launches would mislead the tuner")
     ap.add_argument("--side", type=int, default=128,
                     help="lattice side of the scene (128 = the 2,097,152-particle workload; "
                          "smaller sides are for profiling captures only)")

@@ -489,8 +489,18 @@ __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
 // Solver rows from the hit rows: G lanes per particle.
 constexpr int kEmitG = 8;
 constexpr int kStash = 128;  // b-only entries kept per group before appending
+// Chunks of kEmitG entries whose loads are issued together, and resident
+// blocks per SM asked of the register allocator: 2 chunks at 8 blocks (32
+// registers) measured fastest at 2M, ahead of 1, 3 or 4 chunks at 4-6 blocks.
+#ifndef PK_EMIT_U
+#define PK_EMIT_U 2
+#endif
+#ifndef PK_EMIT_MINB
+#define PK_EMIT_MINB 8
+#endif
+constexpr int kEmitU = PK_EMIT_U;
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, PK_EMIT_MINB)
     k_emit(const int* __restrict__ hcnt, const uint2* __restrict__ hits, const uint2* __restrict__ tau,
            const int* __restrict__ perm, int n, int cap, int row_cap, int* __restrict__ rows,
            int2* __restrict__ rcnt, int* __restrict__ pub_index, int* __restrict__ pub_elements,
@@ -522,43 +532,59 @@ __global__ void __launch_bounds__(256)
     for (int o = 16; o >= 1; o >>= 1) cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
     int nA = 0, nB = 0;
     bool over = false;
-    for (int e0 = 0; e0 < cmax; e0 += kEmitG) {
-        const int e = e0 + sub;
-        bool fa = false, fb = false;
-        int t = 0;
-        if (valid && e < cnt) {
-            const uint2 h = __ldg(hrow + e);
-            t = (int)h.x;
-            if (capped) {
-                const float d2 = __uint_as_float(h.y);
-                fa = key_le(d2, t, ti);
-                fb = key_le(d2, s, __ldg(tau + t));
-            } else {
-                fa = fb = true;
-            }
+    // kEmitU chunks per round: their hit loads, then their tau_j gathers, are
+    // all in flight before the first ballot (the chunks are then decided and
+    // written in order, as one chunk at a time would)
+    for (int e0 = 0; e0 < cmax; e0 += kEmitG * kEmitU) {
+        uint2 h[kEmitU], tj[kEmitU];
+#pragma unroll
+        for (int u = 0; u < kEmitU; ++u) {
+            const int e = e0 + u * kEmitG + sub;
+            h[u] = (valid && e < cnt) ? __ldg(hrow + e) : make_uint2(0u, 0u);
         }
-        const unsigned ba = __ballot_sync(kFull, fa) & gmask;
-        const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
-        if (fa) {
-            const int q = nA + __popc(ba & lt_g);
-            rows[row_slot(so, q, row_cap)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
-            if (pub) {
-                const long long o = pbase + q;
-                if (capped ? (q < cap) : (o < pub_capacity))
-                    pub_elements[o] = __ldg(perm + t);
+#pragma unroll
+        for (int u = 0; u < kEmitU; ++u) {
+            const int e = e0 + u * kEmitG + sub;
+            tj[u] = (capped && valid && e < cnt) ? __ldg(tau + h[u].x) : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < kEmitU; ++u) {
+            if (e0 + u * kEmitG >= cmax) break;  // warp-uniform: cmax is the warp's maximum
+            const int e = e0 + u * kEmitG + sub;
+            bool fa = false, fb = false;
+            const int t = (int)h[u].x;
+            if (valid && e < cnt) {
+                if (capped) {
+                    const float d2 = __uint_as_float(h[u].y);
+                    fa = key_le(d2, t, ti);
+                    fb = key_le(d2, s, tj[u]);
+                } else {
+                    fa = fb = true;
+                }
+            }
+            const unsigned ba = __ballot_sync(kFull, fa) & gmask;
+            const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
+            if (fa) {
+                const int q = nA + __popc(ba & lt_g);
+                rows[row_slot(so, q, row_cap)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
+                if (pub) {
+                    const long long o = pbase + q;
+                    if (capped ? (q < cap) : (o < pub_capacity))
+                        pub_elements[o] = __ldg(perm + t);
+                    else
+                        over = true;
+                }
+            }
+            if (fb && !fa) {
+                const int q = nB + __popc(bb & lt_g);
+                if (q < kStash)
+                    s_b[grp][q] = t | kRowFlagB;
                 else
                     over = true;
             }
+            nA += __popc(ba);
+            nB += __popc(bb);
         }
-        if (fb && !fa) {
-            const int q = nB + __popc(bb & lt_g);
-            if (q < kStash)
-                s_b[grp][q] = t | kRowFlagB;
-            else
-                over = true;
-        }
-        nA += __popc(ba);
-        nB += __popc(bb);
     }
     __syncwarp();
     if (valid) {
