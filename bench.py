@@ -585,21 +585,19 @@ def run_pk(args):
     ms_max = max_over_ranks(ms)
     value = world * n * args.steps / (ms_max / 1e3)
 
-    # ---- end to end through the public call with host buffers
+    # ---- end to end through the C-ABI call on host buffers (pk_pbf_step_host:
+    # every frame copies x, v in from page-locked memory and the results back)
     e2e_steps = max(3, min(args.steps, 20))
     xh = torch.empty((n, 3), dtype=torch.float32).pin_memory()
     vh = torch.empty((n, 3), dtype=torch.float32).pin_memory()
     xh.copy_(x.cpu())
     vh.copy_(v.cpu())
+    ctx.pbf_step_host(xh, vh, prm)  # untimed: sizes the context's device copies
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(e2e_steps):
-        x.copy_(xh, non_blocking=True)
-        v.copy_(vh, non_blocking=True)
-        ctx.pbf_step(x, v, prm)
-        xh.copy_(x, non_blocking=True)
-        vh.copy_(v, non_blocking=True)
+        ctx.pbf_step_host(xh, vh, prm)
     f1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(f0.elapsed_time(f1))
@@ -632,7 +630,7 @@ def run_pk(args):
         "step_roofline": {"bytes_per_particle_step": step_bytes, "frac": step_frac,
                           "peak_source": peak_kind},
         "kernel_ms": {k: {"total_ms": prof[k][0], "launches": prof[k][1]} for k in prof},
-        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+        "e2e": {"value": e2e_val, "unit": UNIT, "api": "pk_pbf_step_host", "h2d_bytes_per_step": 2 * n * 12,
                 "d2h_bytes_per_step": 2 * n * 12, "steps": e2e_steps},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,

@@ -207,6 +207,15 @@ typedef struct {
 int pk_pbf_step(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p,
                 float* rho_out, pk_stream stream);
 
+/* pk_pbf_step on host arrays, the view of an application that owns its
+ * particles on the host and reads every frame back (the reference's
+ * ParticleSystem loading and ParticleWriter dumps, ParticleWriter.cpp:49-80).
+ * x, v: n AoS float triples in host memory, updated in place; page-locked
+ * memory gives full PCIe speed.  Copies them into context-owned device arrays
+ * (grown on first use of a larger n), runs the frame and copies the results
+ * back, all on `stream`, then synchronises the stream. */
+int pk_pbf_step_host(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p, pk_stream stream);
+
 /* Many independent scenes in one frame (no reference counterpart; the
  * reference steps each ParticleFluid node with its own launches).  The scenes'
  * particles are concatenated in caller order: scene s owns particles

@@ -250,7 +250,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
-                    c->pd_in_cnt, c->pd_in_off, c->pd_in};
+                    c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v};
     pk::pd_work_release(c);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -784,6 +784,37 @@ PK_API int pk_pbf_step(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params
                        pk_stream stream)
 {
     return pbf_step_impl(c, x, v, n, p, rho_out, nullptr, 1, stream, "pk_pbf_step");
+}
+
+PK_API int pk_pbf_step_host(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (n < 0 || (n > 0 && (!x || !v)) || !p) return fail(c, PK_ERR_ARG, "pk_pbf_step_host: bad arguments");
+    cudaSetDevice(c->device);
+    if (n > c->h_cap) {
+        if (!(regrow(c->h_x, 3 * (size_t)n) && regrow(c->h_v, 3 * (size_t)n))) {
+            c->h_cap = 0;
+            return fail(c, PK_ERR_NOMEM, "pk_pbf_step_host: out of device memory");
+        }
+        c->h_cap = n;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = sizeof(float) * 3 * (size_t)n;
+    cudaError_t e = cudaSuccess;
+    if (n > 0) {
+        e = cudaMemcpyAsync(c->h_x, x, bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->h_v, v, bytes, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(c, e, "pk_pbf_step_host: copy in");
+    }
+    int rc = pbf_step_impl(c, c->h_x, c->h_v, n, p, nullptr, nullptr, 1, stream, "pk_pbf_step_host");
+    if (rc != PK_OK) return rc;
+    if (n > 0) {
+        e = cudaMemcpyAsync(x, c->h_x, bytes, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(v, c->h_v, bytes, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(c, e, "pk_pbf_step_host: copy out");
+    }
+    return PK_OK;
 }
 
 PK_API int pk_pbf_step_batched(pk_ctx* c, float* x, float* v, const int* scene_offsets, int nscenes,

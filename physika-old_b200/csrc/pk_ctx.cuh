@@ -57,6 +57,10 @@ struct pk_ctx {
     float* g_lam = nullptr;
     float* g_dpos = nullptr;  // 3 per particle
     float* g_xold = nullptr;  // 3 per particle
+    // device copies of the caller's host arrays (pk_pbf_step_host)
+    float* h_x = nullptr;  // 3 per particle
+    float* h_v = nullptr;  // 3 per particle
+    int h_cap = 0;
 
     // ---- state of the last neighbour build
     pk::Grid grid{};

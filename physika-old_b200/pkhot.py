@@ -19,7 +19,7 @@ EXPORTED = [
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
     "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain", "pk_viscosity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
-    "pk_pbf_step_batched",
+    "pk_pbf_step_batched", "pk_pbf_step_host",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
     "pk_pd_compute_inverse_k", "pk_pd_begin", "pk_pd_enforce", "pk_pd_update_velocity",
     "pk_pd_rotate_rest_shape", "pk_pd_apply_yielding", "pk_pd_reconstruct_rest_shape", "pk_pd_fracture",
@@ -98,6 +98,7 @@ def load():
         "pk_boundary_jitter": ([P, I, P, P], I),
         "pk_pbf_step": ([P, P, P, I, ctypes.POINTER(PbfParams), P, P], I),
         "pk_pbf_step_batched": ([P, P, P, P, I, I, ctypes.POINTER(PbfParams), P, P], I),
+        "pk_pbf_step_host": ([P, P, P, I, ctypes.POINTER(PbfParams), P], I),
         "pk_pd_init": ([P, P, I, P, P, I, LL, F, P], I),
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
@@ -309,6 +310,16 @@ class Context:
     def pbf_step(self, x, v, params, rho_out=None):
         self._check(self.L.pk_pbf_step(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(params),
                                        _ptr(rho_out), _stream()))
+
+    def pbf_step_host(self, x, v, params):
+        """pbf_step on contiguous float32 CPU tensors (n, 3), updated in place;
+        pinned tensors give full PCIe speed.  Returns after the copies back."""
+        import torch
+        for t in (x, v):
+            if t.is_cuda or not t.is_contiguous() or t.dtype != torch.float32 or t.shape != x.shape:
+                raise ValueError("expected a contiguous float32 CPU tensor")
+        self._check(self.L.pk_pbf_step_host(self.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(v.data_ptr()),
+                                            x.shape[0], ctypes.byref(params), _stream()))
 
     def pbf_step_batched(self, x, v, scene_offsets, params, rho_out=None):
         """One frame of len(scene_offsets) - 1 independent scenes concatenated in x, v."""

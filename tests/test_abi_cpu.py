@@ -36,6 +36,7 @@ def test_argument_errors_need_no_device():
     L = pkhot.load()
     assert L.pk_ctx_destroy(None) == pkhot.PK_ERR_ARG
     assert L.pk_ctx_create(None, 0) == pkhot.PK_ERR_ARG
+    assert L.pk_pbf_step_host(None, None, None, 0, None, None) == pkhot.PK_ERR_ARG
     p = pkhot.nq_params(0.01, (0, 0, 0), (1, 1, 1), 60)
     assert L.pk_nq_build(None, None, 0, ctypes.byref(p), None, None, 0, None, None) == pkhot.PK_ERR_ARG
     assert L.pk_last_error(None) == b"null context"
