@@ -250,7 +250,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
-                    c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v};
+                    c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v, c->pd_ktw, c->pl_mk};
     pk::pd_work_release(c);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -864,7 +864,7 @@ PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const 
     if (n > c->pd_cap_n) {
         size_t m = (size_t)n;
         if (!(regrow(c->pd_index, m) && regrow(c->pd_invK, 9 * m) && regrow(c->pd_bulk, m) &&
-              regrow(c->pd_xold, 3 * m) && regrow(c->pd_delta, 3 * m) && regrow(c->pd_w, m) &&
+              regrow(c->pd_xold, 3 * m) && regrow(c->pd_delta, 3 * m) && regrow(c->pd_w, m) && regrow(c->pd_ktw, m) &&
               regrow(c->pd_in_cnt, m + 1) && regrow(c->pd_in_off, m + 1))) {
             c->pd_cap_n = 0;
             return fail(c, PK_ERR_NOMEM, "device allocation of elasticity state failed");
@@ -1042,7 +1042,8 @@ int ensure_plastic(pk_ctx* c)
     if (n <= c->pl_cap_n && c->pl_y1) return PK_OK;
     const size_t m = (size_t)std::max(n, 1);
     if (!(regrow(c->pl_y1, m) && regrow(c->pl_y2, m) && regrow(c->pl_i1, m) && regrow(c->pl_yield, m) &&
-          regrow(c->pl_invF, 9 * m) && regrow(c->pl_sizes, m + 1) && regrow(c->pl_off, m + 1))) {
+          regrow(c->pl_invF, 9 * m) && regrow(c->pl_mk, (size_t)pk::kPlMk * m) && regrow(c->pl_sizes, m + 1) &&
+          regrow(c->pl_off, m + 1))) {
         c->pl_cap_n = 0;
         return fail(c, PK_ERR_NOMEM, "device allocation of the plasticity state failed");
     }
@@ -1113,6 +1114,7 @@ PK_API int pk_pd_rotate_rest_shape(pk_ctx* c, const float* x, int n, float horiz
     if (!(horizon > 0.0f)) return fail(c, PK_ERR_ARG, "horizon must be positive");
     if (n > 0 && !x) return fail(c, PK_ERR_ARG, "null positions");
     cudaSetDevice(c->device);
+    if ((rc = ensure_plastic(c))) return rc;
     c->launches = pk::pl_rotate(c, x, horizon, (cudaStream_t)stream);
     return check_launch(c, "pk_pd_rotate_rest_shape");
 }

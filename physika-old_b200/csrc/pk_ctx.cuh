@@ -96,6 +96,7 @@ struct pk_ctx {
     float* pd_xold = nullptr;
     float* pd_delta = nullptr;
     float* pd_w = nullptr;
+    float* pd_ktw = nullptr;  // computeInverseK: the weight sum between its two kernels
     float pd_horizon = 0.0f;
     long long pd_cap_bonds = 0;    // capacity of pd_alive and pd_in
     long long pd_cap_rest = 0;     // capacity of pd_rest_idx / pd_rest_pos
@@ -108,6 +109,7 @@ struct pk_ctx {
     float* pl_i1 = nullptr;         // m_I1
     unsigned char* pl_yield = nullptr;  // m_bYield
     float* pl_invF = nullptr;       // m_invF, 9 per particle
+    float* pl_mk = nullptr;         // rotateRestShape: sums, then the rotation (kPlMk per particle)
     int* pl_sizes = nullptr;        // n + 1
     int* pl_off = nullptr;          // n + 1
     int* pl_rest_idx2 = nullptr;

@@ -59,6 +59,7 @@ int pd_begin(pk_ctx* c, const float* x, int n, float horizon, float mu, float la
 int pd_enforce(pk_ctx* c, float* x, int n, float horizon, float mu, float lambda, cudaStream_t st);
 int pd_update_velocity(pk_ctx* c, const float* x, float* v, int n, float dt, cudaStream_t st);
 // pk_plastic.cu
+constexpr int kPlMk = 20;  // floats per particle of the rotation scratch (pk_ctx::pl_mk)
 int pl_rotate(pk_ctx* c, const float* x, float h, cudaStream_t st);
 int pl_yield(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t st);
 int pl_fracture(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t st);

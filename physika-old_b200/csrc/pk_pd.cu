@@ -45,31 +45,52 @@ __global__ void __launch_bounds__(256)
 // EM_PrecomputeShape (ElasticityModule.cu:21-116): weighted second moment of
 // the rest bonds, then the pseudo-inverse with singular values <= 1e-4*h
 // replaced by 1 (polarDecomposition's SVD of a symmetric PSD matrix is its
-// eigen-decomposition).  invK row-major.
+// eigen-decomposition).  invK row-major.  Two kernels: eight lanes per
+// particle sum the bonds (coalesced walks of the rest shape) into invK and
+// tws, then one thread per particle takes the eigen-decomposition in place
+// (every lane of a warp busy with its own double-precision solve).
 __global__ void __launch_bounds__(128)
-    k_pd_invk(int n, const int* __restrict__ index, int cap, long long total,
-              const float* __restrict__ rpos, float h, float* __restrict__ invK)
+    k_pd_invk_sums(int n, const int* __restrict__ index, int cap, long long total,
+                   const float* __restrict__ rpos, float h, float* __restrict__ Kout, float* __restrict__ tws)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    long long a0 = pd_at(index, cap, i, 0);
-    float ri0 = rpos[3 * a0], ri1 = rpos[3 * a0 + 1], ri2 = rpos[3 * a0 + 2];
-    int m = pd_size(index, cap, total, n, i);
+    const Lane8 L = lane8_of(n);
+    const int i = L.i;
+    const long long a0 = pd_at(index, cap, i, 0);
+    const float ri0 = rpos[3 * a0], ri1 = rpos[3 * a0 + 1], ri2 = rpos[3 * a0 + 2];
+    const int m = pd_size(index, cap, total, n, i);
     float M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, tw = 0.f;
-    for (int e = 0; e < m; ++e) {
-        long long at = pd_at(index, cap, i, e);
-        float q0 = rpos[3 * at] - ri0, q1 = rpos[3 * at + 1] - ri1, q2 = rpos[3 * at + 2] - ri2;
-        float r = sqrtf(q0 * q0 + q1 * q1 + q2 * q2);
+    for (int e = L.sub; e < m; e += 8) {
+        const long long at = pd_at(index, cap, i, e);
+        const float q0 = rpos[3 * at] - ri0, q1 = rpos[3 * at + 1] - ri1, q2 = rpos[3 * at + 2] - ri2;
+        const float r = sqrtf(q0 * q0 + q1 * q1 + q2 * q2);
         if (r > kEpsilon) {
-            float wt = corr_w(r, h), sw = sqrtf(wt);
-            float q[3] = {q0 / h * sw, q1 / h * sw, q2 / h * sw};
+            const float wt = corr_w(r, h), sw = sqrtf(wt);
+            const float q[3] = {q0 / h * sw, q1 / h * sw, q2 / h * sw};
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) M[a][b] += q[a] * q[b];
             tw += wt;
         }
     }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) M[a][b] = sum8(M[a][b]);
+    tw = sum8(tw);
+    if (!L.valid || L.sub != 0) return;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) Kout[9LL * i + 3 * a + b] = M[a][b];
+    tws[i] = tw;
+}
+
+__global__ void __launch_bounds__(128)
+    k_pd_invk_solve(int n, float h, const float* __restrict__ tws, float* __restrict__ invK)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float M[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) M[a][b] = invK[9LL * i + 3 * a + b];
+    const float tw = tws[i];
     if (tw > kEpsilon) {
-        float s = 1.0f / tw;
+        const float s = 1.0f / tw;
         for (int a = 0; a < 3; ++a)
             for (int b = 0; b < 3; ++b) M[a][b] *= s;
     }
@@ -77,15 +98,24 @@ __global__ void __launch_bounds__(128)
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) A[a][b] = (double)M[a][b];
     jacobi3(A, Q, w);
-    double thr = (double)(0.0001f * h);
+    const double thr = (double)(0.0001f * h);
     for (int a = 0; a < 3; ++a) {
-        double sv = fabs(w[a]);
+        const double sv = fabs(w[a]);
         w[a] = sv > thr ? 1.0 / sv : 1.0;
     }
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b)
             invK[9LL * i + 3 * a + b] =
                 (float)(Q[a][0] * w[0] * Q[b][0] + Q[a][1] * w[1] * Q[b][1] + Q[a][2] * w[2] * Q[b][2]);
+}
+
+static int launch_invk(pk_ctx* c, int n, int cap, long long total, float h, cudaStream_t st)
+{
+    k_pd_invk_sums<<<(unsigned)(((long long)n * 8 + 127) / 128), 128, 0, st>>>(n, c->pd_index, cap, total,
+                                                                              c->pd_rest_pos, h, c->pd_invK,
+                                                                              c->pd_ktw);
+    k_pd_invk_solve<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, h, c->pd_ktw, c->pd_invK);
+    return 2;
 }
 
 __global__ void __launch_bounds__(256) k_fill_f(float* __restrict__ p, long long m, float v)
@@ -135,21 +165,18 @@ int pd_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int*
     long long bonds = cap > 0 ? (long long)n * cap : total;
     cudaMemcpyAsync(c->pd_index, index, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st);
     k_pd_rest<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, c->pd_rest_idx, c->pd_rest_pos);
-    k_pd_invk<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, c->pd_index, cap, total, c->pd_rest_pos,
-                                                          horizon, c->pd_invK);
+    const int l = launch_invk(c, n, cap, total, horizon, st);
     k_fill_f<<<nb, 256, 0, st>>>(c->pd_bulk, n, 1.0f);  // computeMaterialStiffness (:371-387)
     if (bonds > 0)
         k_fill_u8<<<(unsigned)((bonds + 255) / 256), 256, 0, st>>>(c->pd_alive, bonds, 1);
-    return 5;
+    return 4 + l;
 }
 
 int pd_inverse_k(pk_ctx* c, float horizon, cudaStream_t st)
 {
     const int n = c->pd_n;
     if (n <= 0) return 0;
-    k_pd_invk<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, c->pd_index, c->pd_cap, c->pd_total, c->pd_rest_pos,
-                                                          horizon, c->pd_invK);
-    return 1;
+    return launch_invk(c, n, c->pd_cap, c->pd_total, horizon, st);
 }
 
 int pd_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float mu, float lambda,

@@ -18,6 +18,31 @@ __device__ __forceinline__ long long pd_at(const int* index, int cap, int i, int
     return cap > 0 ? (long long)cap * i + k : (long long)index[i] + k;
 }
 
+// Eight lanes of one warp per particle (lane `sub` takes bonds sub, sub + 8,
+// ...); the idle lanes of the last group mirror particle n - 1 and write
+// nothing.  sum8 combines a group's partial sums with xor shuffles in a fixed
+// order.
+struct Lane8 {
+    int i, sub;
+    bool valid;
+};
+__device__ __forceinline__ Lane8 lane8_of(int n)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    Lane8 L;
+    L.i = (int)(gid >> 3);
+    L.sub = (int)(gid & 7);
+    L.valid = L.i < n;
+    if (!L.valid) L.i = n - 1;
+    return L;
+}
+__device__ __forceinline__ float sum8(float v)
+{
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // CorrectedKernel / SmoothKernel (Kernel.h:68-75,99-142), float.
 __device__ __forceinline__ float smooth_w(float r, float h)
 {

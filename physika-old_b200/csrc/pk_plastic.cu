@@ -1,9 +1,9 @@
 // pk_plastic.cu -- ElastoplasticityModule and FractureModule
 // (Dynamics/ParticleSystem/ElastoplasticityModule.cu, FractureModule.cu) on
 // the context's peridynamics rest shape.  Every kernel updates only the bonds
-// of its own particle, so the rest shape can be rewritten in place.  The
-// kernels with a double-precision eigen-decomposition per particle run one
-// thread per particle; the others split a particle's bonds over kPlG lanes.
+// of its own particle, so the rest shape can be rewritten in place.  Bond
+// walks split a particle's bonds over kPlG lanes; the double-precision
+// eigen-decompositions run one thread per particle.
 //
 // The reference's SVDs come from svd3_cuda.h (McAdams et al. 2011: U and V
 // rotations, the sign of det A on the smallest singular value).  What the
@@ -165,18 +165,22 @@ __device__ inline float det3f(const float M[3][3])
            M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
 }
 
-// EM_RotateRestShape (ElastoplasticityModule.cu:568-644), one thread per
-// particle (the two double-precision eigen-decompositions dominate, and they
-// keep every lane of a warp busy this way).
-__global__ void __launch_bounds__(128) k_pl_rotate(RestView R, const float* __restrict__ x, float h)
+// EM_RotateRestShape (ElastoplasticityModule.cu:568-644) in three kernels:
+// kPlG lanes per particle sum the deformation moment and the rest-shape
+// moment over the bonds (coalesced walks), one thread per particle forms the
+// rotation (two double-precision eigen-decompositions, every lane of a warp
+// busy with its own particle), and kPlG lanes per particle rotate the bonds.
+// Scratch per particle (kPlMk floats): mat (9), K (9), tw; then R (9).
+__global__ void __launch_bounds__(kPlBlock) k_pl_rot_sums(RestView R, const float* __restrict__ x, float h,
+                                                          float* __restrict__ mk)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R.n) return;
+    const PlLane L = pl_lane(R.n);
+    const int i = L.i;
     const long long a0 = pd_at(R.index, R.cap, i, 0);
     const float ri[3] = {R.rpos[3 * a0], R.rpos[3 * a0 + 1], R.rpos[3 * a0 + 2]};
     const int m = pd_size(R.index, R.cap, R.total, R.n, i);
     float tw = 0.f, mat[3][3] = {}, K[3][3] = {};
-    for (int e = 0; e < m; ++e) {
+    for (int e = L.sub; e < m; e += kPlG) {
         const long long at = pd_at(R.index, R.cap, i, e);
         const int j = R.ridx[at];
         const float* rj = R.rpos + 3 * at;
@@ -196,6 +200,31 @@ __global__ void __launch_bounds__(128) k_pl_rotate(RestView R, const float* __re
             tw += wt;
         }
     }
+    gsum8(mat);
+    gsum8(K);
+    tw = gsum8(tw);
+    if (!L.valid || L.sub != 0) return;
+    float* o = mk + (long long)kPlMk * i;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            o[3 * a + b] = mat[a][b];
+            o[9 + 3 * a + b] = K[a][b];
+        }
+    o[18] = tw;
+}
+
+__global__ void __launch_bounds__(128) k_pl_rot_solve(int n, float h, float* __restrict__ mk)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* o = mk + (long long)kPlMk * i;
+    float mat[3][3], K[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            mat[a][b] = o[3 * a + b];
+            K[a][b] = o[9 + 3 * a + b];
+        }
+    const float tw = o[18];
     if (tw > kEpsilon) {
         const float s = 1.0f / tw;
         for (int a = 0; a < 3; ++a)
@@ -211,10 +240,23 @@ __global__ void __launch_bounds__(128) k_pl_rotate(RestView R, const float* __re
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) Md[a][b] = (double)M2[a][b];
     polar_rotation(Md, Rd);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) o[3 * a + b] = (float)Rd[a][b];
+}
+
+__global__ void __launch_bounds__(kPlBlock) k_pl_rot_apply(RestView R, const float* __restrict__ mk)
+{
+    const PlLane L = pl_lane(R.n);
+    const int i = L.i;
+    const long long a0 = pd_at(R.index, R.cap, i, 0);
+    const float ri[3] = {R.rpos[3 * a0], R.rpos[3 * a0 + 1], R.rpos[3 * a0 + 2]};
+    const int m = pd_size(R.index, R.cap, R.total, R.n, i);
     float Rf[3][3];
     for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) Rf[a][b] = (float)Rd[a][b];
-    for (int e = 0; e < m; ++e) {
+        for (int b = 0; b < 3; ++b) Rf[a][b] = mk[(long long)kPlMk * i + 3 * a + b];
+    __syncwarp();  // every lane holds rest_i before bond 0 (rest_i itself) is rewritten
+    if (!L.valid) return;
+    for (int e = L.sub; e < m; e += kPlG) {
         float* rj = R.rpos + 3 * pd_at(R.index, R.cap, i, e);
         const float d[3] = {rj[0] - ri[0], rj[1] - ri[1], rj[2] - ri[2]};
         for (int a = 0; a < 3; ++a) rj[a] = ri[a] + ((Rf[a][0] * d[0] + Rf[a][1] * d[1]) + Rf[a][2] * d[2]);
@@ -480,8 +522,12 @@ static unsigned blocks(long long m, int b) { return (unsigned)((m + b - 1) / b);
 int pl_rotate(pk_ctx* c, const float* x, float h, cudaStream_t st)
 {
     if (c->pd_n <= 0) return 0;
-    k_pl_rotate<<<blocks(c->pd_n, 128), 128, 0, st>>>(rest_view(c), x, h);
-    return 1;
+    const RestView R = rest_view(c);
+    const unsigned g = blocks((long long)c->pd_n * kPlG, kPlBlock);
+    k_pl_rot_sums<<<g, kPlBlock, 0, st>>>(R, x, h, c->pl_mk);
+    k_pl_rot_solve<<<blocks(c->pd_n, 128), 128, 0, st>>>(c->pd_n, h, c->pl_mk);
+    k_pl_rot_apply<<<g, kPlBlock, 0, st>>>(R, c->pl_mk);
+    return 3;
 }
 
 int pl_yield(pk_ctx* c, const float* x, const pk_plastic_params* p, cudaStream_t st)
