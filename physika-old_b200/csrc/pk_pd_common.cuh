@@ -61,6 +61,11 @@ __device__ __forceinline__ float corr_wrr(float r, float h)
 }
 
 // Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations in double.
+// After four sweeps an off-diagonal element too small to change either
+// diagonal element it couples (|a_pp| + 100 |a_pq| == |a_pp|, likewise a_qq)
+// is set to zero instead of rotated (the threshold rule of Numerical Recipes'
+// jacobi, Press et al.), so the sweeps end once the matrix is diagonal to
+// double precision instead of running on rounding noise.
 __device__ inline void jacobi3(double A[3][3], double Q[3][3], double w[3])
 {
     for (int p = 0; p < 3; ++p)
@@ -71,6 +76,11 @@ __device__ inline void jacobi3(double A[3][3], double Q[3][3], double w[3])
         for (int p = 0; p < 2; ++p)
             for (int q = p + 1; q < 3; ++q) {
                 double apq = A[p][q];
+                const double g = 100.0 * fabs(apq);
+                if (sweep > 3 && fabs(A[p][p]) + g == fabs(A[p][p]) && fabs(A[q][q]) + g == fabs(A[q][q])) {
+                    A[p][q] = A[q][p] = 0.0;
+                    continue;
+                }
                 if (fabs(apq) < 1e-300) continue;
                 double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
                 double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
