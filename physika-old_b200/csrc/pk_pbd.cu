@@ -144,9 +144,19 @@ __global__ void __launch_bounds__(kPassBlock)
 #ifndef PK_PASS_F32X2
 #define PK_PASS_F32X2 1
 #endif
-#ifndef PK_PASS_MINB
-#define PK_PASS_MINB 1
+// Row quads each thread keeps in flight ahead of the one it works on.
+#ifndef PK_PASS_PF
+#define PK_PASS_PF 2
 #endif
+constexpr int kPassPrefetch = PK_PASS_PF;
+#ifndef PK_PASS_WARPS
+#define PK_PASS_WARPS 0  // resident warps per SM asked of the register allocator (0: none)
+#endif
+template <int BLOCK>
+constexpr int pass_min_blocks()
+{
+    return PK_PASS_WARPS > 0 && PK_PASS_WARPS / (BLOCK / 32) > 0 ? PK_PASS_WARPS / (BLOCK / 32) : 1;
+}
 
 struct Geom2 {
     float2 dx, dy, dz, d2, ir, dd;
@@ -200,7 +210,7 @@ __device__ __forceinline__ void dens_one(const float4& a, const float4& xi, cons
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
+__global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
     k_pass_density2(const float4* __restrict__ xs, const int* __restrict__ rows,
                     const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
                     float4* __restrict__ xl, float* __restrict__ rho_out)
@@ -212,10 +222,14 @@ __global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     DensAcc a{};
     const int nfull = na >> 2, nq = (na + 3) >> 2;
-    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    int4 ring[kPassPrefetch];  // ring[k] = quad q + k of the row
+#pragma unroll
+    for (int k = 0; k < kPassPrefetch; ++k) ring[k] = k < nq ? row_quad(rq + 32LL * k) : make_int4(0, 0, 0, 0);
     for (int q = 0; q < nfull; ++q) {
-        const int4 cur = nxt;
-        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));  // next quad in flight
+        const int4 cur = ring[0];
+#pragma unroll
+        for (int k = 0; k + 1 < kPassPrefetch; ++k) ring[k] = ring[k + 1];
+        if (q + kPassPrefetch < nq) ring[kPassPrefetch - 1] = row_quad(rq + 32LL * (q + kPassPrefetch));
         const float4 x0 = __ldg(xs + (cur.x & kRowIndexMask)), x1 = __ldg(xs + (cur.y & kRowIndexMask));
         const float4 x2 = __ldg(xs + (cur.z & kRowIndexMask)), x3 = __ldg(xs + (cur.w & kRowIndexMask));
         dens_pair(x0, x1, xi, k_, a);
@@ -223,7 +237,7 @@ __global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
     }
     const int rest = na - 4 * nfull;
     if (rest > 0) {
-        const int ent[3] = {nxt.x, nxt.y, nxt.z};
+        const int ent[3] = {ring[0].x, ring[0].y, ring[0].z};
 #pragma unroll
         for (int k = 0; k < 3; ++k)
             if (k < rest) dens_one(__ldg(xs + (ent[k] & kRowIndexMask)), xi, k_, a);
@@ -269,7 +283,7 @@ __device__ __forceinline__ void disp_one(const float4& a, int v, const float4& x
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
+__global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
     k_pass_disp2(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
                  int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
 {
@@ -280,10 +294,14 @@ __global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     DispAcc a{};
     const int nfull = nu >> 2, nq = (nu + 3) >> 2;
-    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    int4 ring[kPassPrefetch];  // ring[k] = quad q + k of the row
+#pragma unroll
+    for (int k = 0; k < kPassPrefetch; ++k) ring[k] = k < nq ? row_quad(rq + 32LL * k) : make_int4(0, 0, 0, 0);
     for (int q = 0; q < nfull; ++q) {
-        const int4 cur = nxt;
-        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));  // next quad in flight
+        const int4 cur = ring[0];
+#pragma unroll
+        for (int k = 0; k + 1 < kPassPrefetch; ++k) ring[k] = ring[k + 1];
+        if (q + kPassPrefetch < nq) ring[kPassPrefetch - 1] = row_quad(rq + 32LL * (q + kPassPrefetch));
         const float4 x0 = __ldg(xl + (cur.x & kRowIndexMask)), x1 = __ldg(xl + (cur.y & kRowIndexMask));
         const float4 x2 = __ldg(xl + (cur.z & kRowIndexMask)), x3 = __ldg(xl + (cur.w & kRowIndexMask));
         disp_pair(x0, x1, cur.x, cur.y, xi, k_, a);
@@ -291,7 +309,7 @@ __global__ void __launch_bounds__(BLOCK, PK_PASS_MINB)
     }
     const int rest = nu - 4 * nfull;
     if (rest > 0) {
-        const int ent[3] = {nxt.x, nxt.y, nxt.z};
+        const int ent[3] = {ring[0].x, ring[0].y, ring[0].z};
 #pragma unroll
         for (int k = 0; k < 3; ++k)
             if (k < rest) disp_one(__ldg(xl + (ent[k] & kRowIndexMask)), ent[k], xi, k_, a);
@@ -357,10 +375,14 @@ __global__ void __launch_bounds__(BLOCK)
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     float tw = 0.f, dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
     const int nq = (na + 3) >> 2;
-    int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
+    int4 ring[kPassPrefetch];  // ring[k] = quad q + k of the row
+#pragma unroll
+    for (int k = 0; k < kPassPrefetch; ++k) ring[k] = k < nq ? row_quad(rq + 32LL * k) : make_int4(0, 0, 0, 0);
     for (int q = 0; q < nq; ++q) {
-        const int4 cur = nxt;
-        if (q + 1 < nq) nxt = row_quad(rq + 32LL * (q + 1));
+        const int4 cur = ring[0];
+#pragma unroll
+        for (int k = 0; k + 1 < kPassPrefetch; ++k) ring[k] = ring[k + 1];
+        if (q + kPassPrefetch < nq) ring[kPassPrefetch - 1] = row_quad(rq + 32LL * (q + kPassPrefetch));
         const int ent[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
