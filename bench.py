@@ -686,6 +686,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes comparison")
     ap.add_argument("--no-pd", action="store_true", help="skip the peridynamics bar")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable rollout")
+    ap.add_argument("--pd-only", action="store_true",
+                    help="run only the elastic bar (524,288 particles) and print its dict; for profiler "
+                         "captures of the peridynamics step")
     ap.add_argument("--elastoplastic-only", action="store_true",
                     help="run only the elastoplastic frame (65,536 particles) and print its dict; for "
                          "profiler captures of that frame")
@@ -699,6 +702,11 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.pd_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(measure_pd(0, args.steps, args.warmup, torch.cuda.synchronize)), flush=True)
+        return 0
     if args.elastoplastic_only:
         import torch
         torch.cuda.set_device(0)
