@@ -113,7 +113,8 @@ int pk_summation_density(pk_ctx* ctx, const float* x, int n, const int* index,
  * in place; rho_out (may be NULL) receives outDensity.  When (index, elements)
  * are the arrays the last pk_nq_build on this context wrote (and n matches),
  * the solve runs on the context's sorted internal list; any other list is
- * solved as given. */
+ * solved as given, and a neighbour id in it outside [0, n) is skipped and
+ * reported by pk_ctx_status as PK_ERR_ARG. */
 int pk_pbd_solve(pk_ctx* ctx, float* x, float* v, int n, const int* index,
                  const int* elements, int cap, long long total,
                  const pk_pbd_params* p, float* rho_out, pk_stream stream);
@@ -230,6 +231,22 @@ int pk_pbf_step_host(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params
  * CUDA graph. */
 int pk_pbf_step_batched(pk_ctx* ctx, float* x, float* v, const int* scene_offsets, int nscenes, int n,
                         const pk_pbf_params* p, float* rho_out, pk_stream stream);
+
+/* A frame as a CUDA graph (no reference counterpart).  pk_graph_capture
+ * records one frame -- pk_pbf_step when nscenes == 1 (scene_offsets may be
+ * NULL), else pk_pbf_step_batched -- with these arguments into a graph the
+ * context owns, replacing any earlier one.  It first runs that frame once
+ * on `stream` without capture, so every buffer the frame needs exists before
+ * recording (a captured frame allocates nothing); x and v therefore advance by
+ * one frame.  pk_graph_launch replays the recorded frame on `stream`: the
+ * same kernels on the same pointers and parameters, one launch for the whole
+ * frame.  The context's autotuning trials and profiling must be off while a
+ * frame is captured (PK_ERR_STATE otherwise).  pk_graph_release frees the
+ * graph; pk_ctx_destroy does too. */
+int pk_graph_capture(pk_ctx* ctx, float* x, float* v, const int* scene_offsets, int nscenes, int n,
+                     const pk_pbf_params* p, float* rho_out, pk_stream stream);
+int pk_graph_launch(pk_ctx* ctx, pk_stream stream);
+int pk_graph_release(pk_ctx* ctx);
 
 /* Number of kernel launches the last pk_pbf_step enqueued. */
 int pk_last_launch_count(const pk_ctx* ctx);
@@ -398,11 +415,13 @@ int pk_pd_rollout_backward_f64(pk_ctx* ctx, const double* xbar, const double* vb
  * all.  Its scratch is one fixed device array inside the library (4 MiB, held
  * by every GPU that loads the library until exit), so n may be at most
  * pk_noalloc_max_particles() (131072); larger n returns PK_ERR_CAPACITY.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array: calls
- * whose work overlaps on the GPU (different streams, or several host threads)
- * race on it and must be ordered by the caller.  Nothing is allocated or
- * freed. */
+ * The first call in a CUDA context looks up the array's device address (an
+ * address belongs to the context, so a call under another context, or after
+ * cudaDeviceReset, looks it up again); make that first call before any stream
+ * capture.  All calls share the array: calls whose work overlaps on the GPU
+ * (different streams, or several host threads) race on it and must be ordered
+ * by the caller.  A neighbour id outside [0, n) is skipped (there is no
+ * context to report it).  Nothing is allocated or freed. */
 int pk_noalloc_max_particles(void);
 int pk_pbd_solve_noalloc(float* x, float* v, int n, const int* index, const int* elements,
                          int cap, long long total, const pk_pbd_params* p, float* rho_out,

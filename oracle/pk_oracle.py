@@ -94,10 +94,12 @@ def set_norm_variant(v):
 
 
 def set_threads(t):
+    """OpenMP threads of the restatement; t <= 0 means one per host processor."""
     lib().pko_set_threads(int(t))
 
 
 def max_threads():
+    """Threads the next parallel region will use (as last set)."""
     return lib().pko_max_threads()
 
 

@@ -59,17 +59,22 @@ def build_framework(force=False, verbose=True):
     return out
 
 
-REFERENCE = os.environ.get("PK_REFERENCE_SRC", "/root/reference")
+# The reference checkout: PK_REFERENCE_SRC, else a directory named `reference`
+# beside this repository.  Only the golden-fixture drivers under oracle/_ref
+# need it; a machine without it uses the prebuilt drivers.
+REFERENCE = os.environ.get("PK_REFERENCE_SRC") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def build_oracle(verbose=True, with_ref=False):
-    """The CPU restatement; with_ref also builds the golden-vector driver
-    oracle/_ref/ref_math_probe from the reference sources when they are present
-    (they are not on a GPU machine, which uses the prebuilt driver)."""
+    """The CPU restatement; with_ref also builds the golden-fixture drivers from
+    the reference sources when they are present: oracle/_ref/ref_math_probe
+    (its vector math and kernel weights) and oracle/_ref/pkref_driver (its own
+    NeighborQuery, SummationDensity, DensityPBD, ParticleIntegrator and
+    ElasticityModule kernels)."""
     out = None if verbose else subprocess.DEVNULL
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True, stdout=out)
     if with_ref and os.path.isdir(os.path.join(REFERENCE, "Source")):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + REFERENCE],
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref", "refk", "REF=" + REFERENCE],
                        check=True, stdout=out)
 
 

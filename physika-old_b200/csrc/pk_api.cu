@@ -237,10 +237,14 @@ PK_API int pk_ctx_create(pk_ctx** out, int device)
     return PK_OK;
 }
 
+PK_API int pk_graph_release(pk_ctx* c);
+
 PK_API int pk_ctx_destroy(pk_ctx* c)
 {
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
+    pk_graph_release(c);
+    if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
     for (auto& e : c->tune.ev)
         if (e) cudaEventDestroy(e);
     void* ptrs[] = {c->d_err, c->perm, c->inv, c->key, c->rank, c->count, c->count_c, c->offs,
@@ -278,7 +282,7 @@ PK_API int pk_ctx_status(pk_ctx* c, pk_stream stream)
         cudaMemset(c->d_err, 0, sizeof(int));
         char msg[160];
         if (bits & pk::kErrBadIndex) {
-            snprintf(msg, sizeof msg, "a particle id outside [0, n) was given (flags 0x%x)", bits);
+            snprintf(msg, sizeof msg, "a particle id outside [0, n) was given in pins or a neighbour list (flags 0x%x)", bits);
             return fail(c, PK_ERR_ARG, msg);
         }
         snprintf(msg, sizeof msg, "capacity exceeded on the device (flags 0x%x: 1=row, 2=hits>512, 4=list)", bits);
@@ -443,7 +447,7 @@ PK_API int pk_summation_density(pk_ctx* c, const float* x, int n, const int* ind
     if (n > 0 && (!x || !rho)) return fail(c, PK_ERR_ARG, "null positions or density");
     cudaSetDevice(c->device);
     pk::density_generic(x, n, index, elements, cap, total, pk::make_spiky(p->smoothing_length),
-                        effective_mass(p), rho, (cudaStream_t)stream);
+                        effective_mass(p), rho, c->d_err, (cudaStream_t)stream);
     return check_launch(c, "pk_summation_density");
 }
 
@@ -824,6 +828,73 @@ PK_API int pk_pbf_step_batched(pk_ctx* c, float* x, float* v, const int* scene_o
     if (nscenes < 1 || (nscenes > 1 && !scene_offsets))
         return fail(c, PK_ERR_ARG, "need at least one scene and its offsets");
     return pbf_step_impl(c, x, v, n, p, rho_out, scene_offsets, nscenes, stream, "pk_pbf_step_batched");
+}
+
+// ======================================================================
+// a frame recorded as a CUDA graph
+
+PK_API int pk_graph_release(pk_ctx* c)
+{
+    if (!c) return PK_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    return PK_OK;
+}
+
+PK_API int pk_graph_capture(pk_ctx* c, float* x, float* v, const int* scene_offsets, int nscenes, int n,
+                            const pk_pbf_params* p, float* rho_out, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (nscenes < 1 || (nscenes > 1 && !scene_offsets))
+        return fail(c, PK_ERR_ARG, "need at least one scene and its offsets");
+    if (c->tune.on || c->prof) return fail(c, PK_ERR_STATE, "autotuning or profiling is on");
+    cudaSetDevice(c->device);
+    pk_graph_release(c);
+    // one frame as usual: grows every buffer the frame touches
+    int rc = pbf_step_impl(c, x, v, n, p, rho_out, nscenes > 1 ? scene_offsets : nullptr, nscenes, stream,
+                           "pk_graph_capture");
+    if (rc != PK_OK) return rc;
+    cudaError_t e = cudaSuccess;
+    if (!c->capture_stream) e = cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking);
+    // the capture stream starts after the warm frame
+    cudaEvent_t ready = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ready, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->capture_stream, ready, 0);
+    if (ready) cudaEventDestroy(ready);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(c->capture_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_graph_capture: begin");
+    rc = pbf_step_impl(c, x, v, n, p, rho_out, nscenes > 1 ? scene_offsets : nullptr, nscenes,
+                       (pk_stream)c->capture_stream, "pk_graph_capture");
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(c->capture_stream, &g);
+    if (rc != PK_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_graph_capture: end");
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(c, e, "pk_graph_capture: instantiate");
+    }
+    c->graph = g;
+    c->graph_exec = ex;
+    return PK_OK;
+}
+
+PK_API int pk_graph_launch(pk_ctx* c, pk_stream stream)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!c->graph_exec) return fail(c, PK_ERR_STATE, "no frame recorded (pk_graph_capture)");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaGraphLaunch(c->graph_exec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pk_graph_launch");
+    return PK_OK;
 }
 
 // ======================================================================

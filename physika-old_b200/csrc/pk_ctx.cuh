@@ -62,6 +62,11 @@ struct pk_ctx {
     float* h_v = nullptr;  // 3 per particle
     int h_cap = 0;
 
+    // ---- a recorded frame (pk_graph_capture)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t capture_stream = nullptr;
+
     // ---- state of the last neighbour build
     pk::Grid grid{};
     int nq_n = -1;

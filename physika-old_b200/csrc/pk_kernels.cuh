@@ -34,11 +34,11 @@ int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, co
 int pbd_generic_solve_scratch(float* x, float* v, int n, const int* index, const int* elements,
                               int cap, long long total, const Spiky& k, float mass, int iterations,
                               float dt, float* rho_out, float* rho_s, float* lam, float* dpos,
-                              float* xold, cudaStream_t st);
+                              float* xold, int* err, cudaStream_t st);
 // pk_api.cu: the mass the density kernels use (SummationDensity scaling).
 float effective_mass_of(const pk_pbd_params* p);
 int density_generic(const float* x, int n, const int* index, const int* elements, int cap,
-                    long long total, const Spiky& k, float mass, float* rho, cudaStream_t st);
+                    long long total, const Spiky& k, float mass, float* rho, int* err, cudaStream_t st);
 int gather_state(pk_ctx* c, const float* x, const float* v, int n, cudaStream_t st);
 int integrate_aos(float* x, float* v, const float* f, int n, const float g[3], float dt,
                   cudaStream_t st);

@@ -562,10 +562,19 @@ __device__ __forceinline__ long long nb_at(const int* index, int cap, int i, int
     return cap > 0 ? (long long)cap * i + k : (long long)index[i] + k;
 }
 
+// A neighbour id of a caller's list outside [0, n) is skipped (never read or
+// scattered to) and latched as kErrBadIndex where the caller gave a flag word.
+__device__ __forceinline__ bool valid_id(int j, int n, int* err)
+{
+    if (j >= 0 && j < n) return true;
+    if (err) atomicOr(err, kErrBadIndex);
+    return false;
+}
+
 __global__ void __launch_bounds__(256)
     k_g_density(const float* __restrict__ x, int n, const int* __restrict__ index,
                 const int* __restrict__ elements, int cap, long long total, Spiky k, float mass,
-                float* __restrict__ rho)
+                float* __restrict__ rho, int* __restrict__ err)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -573,6 +582,7 @@ __global__ void __launch_bounds__(256)
     int m = nb_size(index, cap, total, n, i);
     for (int e = 0; e < m; ++e) {
         int j = elements[nb_at(index, cap, i, e)];
+        if (!valid_id(j, n, err)) continue;
         float dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
         float r = sqrtf(dx * dx + dy * dy + dz * dz), w, g;
         spiky_wg(k, r, w, g);
@@ -584,7 +594,8 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     k_g_lambda(const float* __restrict__ x, const float* __restrict__ rho, int n,
                const int* __restrict__ index, const int* __restrict__ elements, int cap,
-               long long total, Spiky k, float* __restrict__ lam, float* __restrict__ dpos)
+               long long total, Spiky k, float* __restrict__ lam, float* __restrict__ dpos,
+               int* __restrict__ err)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -593,6 +604,7 @@ __global__ void __launch_bounds__(256)
     int m = nb_size(index, cap, total, n, i);
     for (int e = 0; e < m; ++e) {
         int j = elements[nb_at(index, cap, i, e)];
+        if (!valid_id(j, n, err)) continue;
         float dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
         float r = sqrtf(dx * dx + dy * dy + dz * dz);
         if (r > kEpsilon) {
@@ -615,7 +627,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     k_g_disp(const float* __restrict__ x, const float* __restrict__ lam, int n,
              const int* __restrict__ index, const int* __restrict__ elements, int cap,
-             long long total, Spiky k, float* __restrict__ dpos)
+             long long total, Spiky k, float* __restrict__ dpos, int* __restrict__ err)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -623,6 +635,7 @@ __global__ void __launch_bounds__(256)
     int m = nb_size(index, cap, total, n, i);
     for (int e = 0; e < m; ++e) {
         int j = elements[nb_at(index, cap, i, e)];
+        if (!valid_id(j, n, err)) continue;
         float dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
         float r = sqrtf(dx * dx + dy * dy + dz * dz);
         if (r > kEpsilon) {
@@ -656,10 +669,11 @@ __global__ void __launch_bounds__(256)
 }
 
 int density_generic(const float* x, int n, const int* index, const int* elements, int cap,
-                    long long total, const Spiky& k, float mass, float* rho, cudaStream_t st)
+                    long long total, const Spiky& k, float mass, float* rho, int* err, cudaStream_t st)
 {
     if (n <= 0) return 0;
-    k_g_density<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho);
+    k_g_density<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho,
+                                                              err);
     return 1;
 }
 
@@ -667,30 +681,17 @@ int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, co
                       int cap, long long total, const Spiky& k, float mass, int iterations,
                       float dt, float* rho_out, cudaStream_t st)
 {
-    if (n <= 0) return 0;
-    const unsigned nb = (unsigned)((n + 255) / 256);
-    const long long m3 = 3LL * n;
-    const unsigned nb3 = (unsigned)((m3 + 255) / 256);
-    int launches = 0;
-    cudaMemcpyAsync(c->g_xold, x, sizeof(float) * (size_t)m3, cudaMemcpyDeviceToDevice, st);
-    float* rho = rho_out != nullptr ? rho_out : c->g_rho;
-    for (int it = 0; it < iterations; ++it) {
-        k_g_density<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho);
-        k_g_lambda<<<nb, 256, 0, st>>>(x, rho, n, index, elements, cap, total, k, c->g_lam, c->g_dpos);
-        k_g_disp<<<nb, 256, 0, st>>>(x, c->g_lam, n, index, elements, cap, total, k, c->g_dpos);
-        k_g_add<<<nb3, 256, 0, st>>>(x, c->g_dpos, m3);
-        launches += 4;
-    }
-    k_g_velocity<<<nb3, 256, 0, st>>>(v, x, c->g_xold, m3, dt);
-    return launches + 1;
+    return pbd_generic_solve_scratch(x, v, n, index, elements, cap, total, k, mass, iterations, dt, rho_out,
+                                     c->g_rho, c->g_lam, c->g_dpos, c->g_xold, c->d_err, st);
 }
 
-// The same generic solve with caller-supplied scratch (rho_s, lam: n floats;
-// dpos, xold: 3n floats), for the entry point that allocates nothing.
+// The generic solve on caller-supplied scratch (rho_s, lam: n floats; dpos,
+// xold: 3n floats): a context's arrays, or the allocation-free entry point's
+// fixed array. err (nullable) receives kErrBadIndex for list ids outside [0, n).
 int pbd_generic_solve_scratch(float* x, float* v, int n, const int* index, const int* elements,
                               int cap, long long total, const Spiky& k, float mass, int iterations,
                               float dt, float* rho_out, float* rho_s, float* lam, float* dpos,
-                              float* xold, cudaStream_t st)
+                              float* xold, int* err, cudaStream_t st)
 {
     if (n <= 0) return 0;
     const unsigned nb = (unsigned)((n + 255) / 256);
@@ -700,9 +701,9 @@ int pbd_generic_solve_scratch(float* x, float* v, int n, const int* index, const
     cudaMemcpyAsync(xold, x, sizeof(float) * (size_t)m3, cudaMemcpyDeviceToDevice, st);
     float* rho = rho_out != nullptr ? rho_out : rho_s;
     for (int it = 0; it < iterations; ++it) {
-        k_g_density<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho);
-        k_g_lambda<<<nb, 256, 0, st>>>(x, rho, n, index, elements, cap, total, k, lam, dpos);
-        k_g_disp<<<nb, 256, 0, st>>>(x, lam, n, index, elements, cap, total, k, dpos);
+        k_g_density<<<nb, 256, 0, st>>>(x, n, index, elements, cap, total, k, mass, rho, err);
+        k_g_lambda<<<nb, 256, 0, st>>>(x, rho, n, index, elements, cap, total, k, lam, dpos, err);
+        k_g_disp<<<nb, 256, 0, st>>>(x, lam, n, index, elements, cap, total, k, dpos, err);
         k_g_add<<<nb3, 256, 0, st>>>(x, dpos, m3);
         launches += 4;
     }
@@ -822,7 +823,7 @@ SdfView sdf_view(const pk_ctx* c)
 __global__ void __launch_bounds__(256)
     k_g_visc(const float* __restrict__ x, const float* __restrict__ vin, const float* __restrict__ vold,
              float* __restrict__ vout, int n, const int* __restrict__ index, const int* __restrict__ elements,
-             int cap, long long total, ViscK k_)
+             int cap, long long total, ViscK k_, int* __restrict__ err)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -831,6 +832,7 @@ __global__ void __launch_bounds__(256)
     const int m = nb_size(index, cap, total, n, i);
     for (int e = 0; e < m; ++e) {
         const int j = elements[nb_at(index, cap, i, e)];
+        if (!valid_id(j, n, err)) continue;
         float d2, ir, dd;
         pair_geom(xi0 - x[3 * j], xi1 - x[3 * j + 1], xi2 - x[3 * j + 2], k_.inv_h, d2, ir, dd);
         const float w = d2 > kEps2 ? k_.cw * dd : 0.0f;
@@ -857,7 +859,7 @@ int viscosity_generic(pk_ctx* c, const float* x, float* v, int n, const int* ind
     cudaMemcpyAsync(c->g_xold, v, bytes, cudaMemcpyDeviceToDevice, st);
     for (int t = 0; t < iterations; ++t) {
         cudaMemcpyAsync(c->g_dpos, v, bytes, cudaMemcpyDeviceToDevice, st);
-        k_g_visc<<<nb, 256, 0, st>>>(x, c->g_dpos, c->g_xold, v, n, index, elements, cap, total, vk);
+        k_g_visc<<<nb, 256, 0, st>>>(x, c->g_dpos, c->g_xold, v, n, index, elements, cap, total, vk, c->d_err);
     }
     return iterations;
 }

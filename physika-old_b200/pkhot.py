@@ -19,7 +19,7 @@ EXPORTED = [
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
     "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain", "pk_viscosity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
-    "pk_pbf_step_batched", "pk_pbf_step_host",
+    "pk_pbf_step_batched", "pk_pbf_step_host", "pk_graph_capture", "pk_graph_launch", "pk_graph_release",
     "pk_pd_init", "pk_pd_set_bulk", "pk_pd_solve", "pk_pd_get_rest_shape",
     "pk_pd_compute_inverse_k", "pk_pd_begin", "pk_pd_enforce", "pk_pd_update_velocity",
     "pk_pd_rotate_rest_shape", "pk_pd_apply_yielding", "pk_pd_reconstruct_rest_shape", "pk_pd_fracture",
@@ -99,6 +99,9 @@ def load():
         "pk_pbf_step": ([P, P, P, I, ctypes.POINTER(PbfParams), P, P], I),
         "pk_pbf_step_batched": ([P, P, P, P, I, I, ctypes.POINTER(PbfParams), P, P], I),
         "pk_pbf_step_host": ([P, P, P, I, ctypes.POINTER(PbfParams), P], I),
+        "pk_graph_capture": ([P, P, P, P, I, I, ctypes.POINTER(PbfParams), P, P], I),
+        "pk_graph_launch": ([P, P], I),
+        "pk_graph_release": ([P], I),
         "pk_pd_init": ([P, P, I, P, P, I, LL, F, P], I),
         "pk_pd_set_bulk": ([P, P, I, P], I),
         "pk_pd_solve": ([P, P, P, I, ctypes.POINTER(PdParams), P], I),
@@ -326,6 +329,19 @@ class Context:
         self._check(self.L.pk_pbf_step_batched(self.h, _ptr(x), _ptr(v), _ptr(scene_offsets),
                                                scene_offsets.shape[0] - 1, x.shape[0],
                                                ctypes.byref(params), _ptr(rho_out), _stream()))
+
+    def graph_capture(self, x, v, params, scene_offsets=None, rho_out=None):
+        """Records one frame (batched when scene_offsets is given) as a CUDA graph
+        owned by the context; the call also runs that frame once, uncaptured."""
+        ns = 1 if scene_offsets is None else scene_offsets.shape[0] - 1
+        self._check(self.L.pk_graph_capture(self.h, _ptr(x), _ptr(v), _ptr(scene_offsets), ns, x.shape[0],
+                                            ctypes.byref(params), _ptr(rho_out), _stream()))
+
+    def graph_launch(self):
+        self._check(self.L.pk_graph_launch(self.h, _stream()))
+
+    def graph_release(self):
+        self._check(self.L.pk_graph_release(self.h))
 
     # ---- ElasticityModule
     def pd_init(self, x, index, elements, cap, total, horizon):

@@ -56,3 +56,39 @@ def test_batched_arguments(ctx):
     with pytest.raises(pkhot.PkError) as e:
         ctx.pbf_step_batched(x, x.clone(), t(np.array([0], np.int32), np.int32), params(sc))
     assert e.value.code == pkhot.PK_ERR_ARG
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_graph_frames_equal_eager_frames(batched):
+    # pk_graph_capture runs one frame, records the next; every replay is that
+    # frame again on the same buffers, bit for bit as eager frames
+    b = scenes.batched_mix(seed=5, nscenes=6, n_min=200, n_max=2000)
+    sc0 = b.scenes[0]
+    x0 = b.x.copy() if batched else b.x[: b.offsets[1]].copy()
+    v0 = np.random.default_rng(5).normal(0, 0.05, x0.shape).astype(np.float32)
+    prm = params(sc0)
+    off = t(b.offsets, np.int32) if batched else None
+    c1, c2 = pkhot.Context(0), pkhot.Context(0)
+    for c in (c1, c2):
+        c.boundary_set_box(sc0.lo, sc0.hi, sc0.sdf_spacing, True)
+    xe, ve = t(x0), t(v0)
+    xg, vg = t(x0), t(v0)
+    c2.graph_capture(xg, vg, prm, off)
+    for k in range(4):
+        if batched:
+            c1.pbf_step_batched(xe, ve, off, prm)
+        else:
+            c1.pbf_step(xe, ve, prm)
+        if k > 0:
+            c2.graph_launch()
+    torch.cuda.synchronize()
+    c1.check_status()
+    c2.check_status()
+    assert np.array_equal(xe.cpu().numpy(), xg.cpu().numpy())
+    assert np.array_equal(ve.cpu().numpy(), vg.cpu().numpy())
+    c2.graph_release()
+    with pytest.raises(pkhot.PkError) as e:
+        c2.graph_launch()
+    assert e.value.code == pkhot.PK_ERR_STATE
+    c1.close()
+    c2.close()

@@ -149,3 +149,21 @@ def test_fused_step_after_build_with_other_row_stride(oracle):
     xo, vo, _ = oracle.pbd_constrain(xo, vo, ri, re, sc.cap, sc.radius, f * m, 5, sc.dt)
     assert rel(x.cpu().numpy(), xo) < 1e-5
     c2.close()
+
+
+def test_foreign_list_with_bad_id_is_skipped_and_reported(ctx, oracle):
+    # an id outside [0, n) in a caller's list: the kernels' own bounds check
+    # skips it and the context reports PK_ERR_ARG; the other pairs are solved
+    sc, v0 = prepared(oracle, seed=5, n_side=8)
+    n = sc.x.shape[0]
+    ri, re = oracle.neighbor_query(sc.x, sc.radius, sc.lo, sc.hi, 60)
+    bad = re.copy()
+    bad[0 * 60 + ri[0] - 1] = n  # last entry of particle 0's row
+    x, v = t(sc.x), t(v0)
+    prm = pkhot.pbd_params(sc.radius, sc.spacing, 1000.0, 5, sc.dt)
+    ctx.pbd_solve(x, v, t(ri).int(), t(bad).int(), 60, n * 60, prm)
+    with pytest.raises(pkhot.PkError) as e:
+        ctx.check_status()
+    assert e.value.code == pkhot.PK_ERR_ARG
+    ctx.check_status()  # the flag is cleared once reported
+    assert np.all(np.isfinite(x.cpu().numpy()))

@@ -1,12 +1,11 @@
 """Size-independent properties at the benchmark's full size (2,097,152
-particles, cap 64) and the error of the float fused frame against a double
-run of the same method.
-
-At 2M the oracle is too slow to compare entry by entry, so the checks are
-properties: the dynamic list is symmetric; every capped row is the cap-nearest
-subset of the dynamic row (count min(cap, |row|), every kept distance <= every
-dropped one up to float rounding); the Jacobi solve conserves momentum (each
-pair's displacement enters both ends with opposite signs)."""
+particles, cap 64), beside the entry-by-entry comparisons with the CPU
+restatement at that size (test_gpu_parity_at_size.py): the dynamic list is
+symmetric; every capped row is the cap-nearest subset of the dynamic row
+(count min(cap, |row|), every kept distance <= every dropped one up to float
+rounding); the Jacobi solve conserves momentum (each pair's displacement
+enters both ends with opposite signs); and, on a 16^3 block, the float fused
+frame against a double run of the same method."""
 import numpy as np
 import pytest
 import torch
