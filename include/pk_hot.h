@@ -406,6 +406,38 @@ int pk_pd_rollout_f64(pk_ctx* ctx, double* x, double* v, const double* bulk, int
 int pk_pd_rollout_backward_f64(pk_ctx* ctx, const double* xbar, const double* vbar, double* grad_x0,
                                double* grad_v0, double* grad_bulk, pk_stream stream);
 
+/* Differentiable DensityPBD rollout (no reference counterpart: the reference
+ * has no derivatives).  `steps` frames of pk_pbf_step without boundary and
+ * viscosity (p->boundary and p->viscosity must be 0; each frame builds its
+ * list on the frame's start positions, integrates, runs DensityPBD and
+ * updates the velocity), x and v (n AoS, device) updated in place; the state
+ * at the start of every checkpoint_every-th step (0: only the first) is kept
+ * on the context for pk_pbd_rollout_backward.  A frame's list is a step
+ * constant: the derivative is that of the frame map with the list frozen.
+ * Rows hold at most 128 hits per particle (beyond, pk_ctx_status reports
+ * PK_ERR_CAPACITY). */
+int pk_pbd_rollout(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p, int steps,
+                   int checkpoint_every, pk_stream stream);
+
+/* Reverse mode of the last pk_pbd_rollout: given dL/dx_T (xbar) and dL/dv_T
+ * (vbar, may be NULL), writes dL/dx_0 and dL/dv_0 (n AoS).  Each segment is
+ * replayed from its checkpoint keeping every frame's rows and Jacobi iterates,
+ * then every iteration, integration and velocity update is reversed by
+ * hand-written kernels (the derivatives of K_ComputeLambdas' lambda, its
+ * clamp, SummationDensity's density and K_ComputeDisplacement's scatter with
+ * the rows' multiplicities).  The reverse state and its arithmetic are double;
+ * the float iterates are read as given. */
+int pk_pbd_rollout_backward(pk_ctx* ctx, const float* xbar, const float* vbar, float* grad_x0, float* grad_v0,
+                            pk_stream stream);
+
+/* The same rollout and reverse mode in double precision (lists from the
+ * positions rounded to float): the reference run of the gradient checks and
+ * the FP64 run the float frames are compared against. */
+int pk_pbd_rollout_f64(pk_ctx* ctx, double* x, double* v, int n, const pk_pbf_params* p, int steps,
+                       int checkpoint_every, pk_stream stream);
+int pk_pbd_rollout_backward_f64(pk_ctx* ctx, const double* xbar, const double* vbar, double* grad_x0,
+                                double* grad_v0, pk_stream stream);
+
 /* ------------------------------------------- DensityPBD without allocation */
 
 /* No counterpart in the reference.  For callers that may not allocate device

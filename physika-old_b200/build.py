@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["pk_sort.cu", "pk_nbr.cu", "pk_pbd.cu", "pk_pd.cu", "pk_pd_adj.cu", "pk_fixed.cu", "pk_plastic.cu", "pk_api.cu",
+CU_SOURCES = ["pk_sort.cu", "pk_nbr.cu", "pk_pbd.cu", "pk_pd.cu", "pk_pd_adj.cu", "pk_fixed.cu", "pk_plastic.cu", "pk_pbd_adj.cu", "pk_api.cu",
               "pk_noalloc.cu"]
 
 

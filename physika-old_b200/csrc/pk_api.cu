@@ -256,6 +256,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
                     c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v, c->pd_ktw, c->pl_mk};
     pk::pd_work_release(c);
+    pk::pbd_roll_release(c);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& ev : c->prof_ev)
@@ -828,6 +829,88 @@ PK_API int pk_pbf_step_batched(pk_ctx* c, float* x, float* v, const int* scene_o
     if (nscenes < 1 || (nscenes > 1 && !scene_offsets))
         return fail(c, PK_ERR_ARG, "need at least one scene and its offsets");
     return pbf_step_impl(c, x, v, n, p, rho_out, scene_offsets, nscenes, stream, "pk_pbf_step_batched");
+}
+
+// ======================================================================
+// differentiable DensityPBD rollouts
+
+namespace {
+
+// Hits per particle the rollout's rows hold (its frames keep every step's
+// rows for the reverse pass, so they are sized to what fluids reach rather
+// than to the 512-hit bound of pk_pbf_step).
+constexpr int kRollRowCap = 128;
+
+int pbd_roll_check(pk_ctx* c, int n, const pk_pbf_params* p, int steps, int every, const void* x,
+                   const void* v)
+{
+    if (!p) return fail(c, PK_ERR_ARG, "null step parameters");
+    if (n <= 0 || n > (1 << 29)) return fail(c, PK_ERR_ARG, "particle count must be in [1, 2^29]");
+    if (!x || !v) return fail(c, PK_ERR_ARG, "null positions or velocities");
+    if (steps < 0 || every < 0) return fail(c, PK_ERR_ARG, "negative step or checkpoint count");
+    int rc = check_nq(c, &p->nq);
+    if (rc || (rc = check_pbd(c, &p->pbd))) return rc;
+    if (p->boundary || p->viscosity > 0.0f)
+        return fail(c, PK_ERR_ARG, "the differentiable frame has no boundary and no viscosity");
+    if (p->nq.cap > kRollRowCap) return fail(c, PK_ERR_ARG, "cap above the rollout's 128 hits per particle");
+    cudaSetDevice(c->device);
+    const pk::Grid g = pk::make_grid(p->nq.radius, p->nq.lo, p->nq.hi);
+    if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
+        (rc = ensure_rows(c, pk::row_slots(n, kRollRowCap))))
+        return rc;
+    return PK_OK;
+}
+
+template <class T>
+int pbd_rollout_entry(pk_ctx* c, T* x, T* v, int n, const pk_pbf_params* p, int steps, int every,
+                      pk_stream stream, const char* what)
+{
+    if (!c) return PK_ERR_ARG;
+    int rc = pbd_roll_check(c, n, p, steps, every, x, v);
+    if (rc) return rc;
+    const int l = pk::pbd_rollout_impl<T>(c, x, v, n, p, steps, every, kRollRowCap, (cudaStream_t)stream);
+    if (l < 0) return fail(c, PK_ERR_NOMEM, "device allocation of the rollout record failed");
+    c->launches = l;
+    return check_launch(c, what);
+}
+
+template <class T>
+int pbd_backward_entry(pk_ctx* c, const T* xbar, const T* vbar, T* gx, T* gv, pk_stream stream, const char* what)
+{
+    if (!c) return PK_ERR_ARG;
+    if (!xbar || !gx || !gv) return fail(c, PK_ERR_ARG, "null gradient arrays");
+    cudaSetDevice(c->device);
+    const int l = pk::pbd_backward_impl<T>(c, xbar, vbar, gx, gv, (cudaStream_t)stream);
+    if (l == -2) return fail(c, PK_ERR_STATE, "no rollout of this precision recorded on the context");
+    if (l < 0) return fail(c, PK_ERR_NOMEM, "device allocation of the reverse pass failed");
+    c->launches = l;
+    return check_launch(c, what);
+}
+
+}  // namespace
+
+PK_API int pk_pbd_rollout(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, int steps,
+                          int checkpoint_every, pk_stream stream)
+{
+    return pbd_rollout_entry<float>(c, x, v, n, p, steps, checkpoint_every, stream, "pk_pbd_rollout");
+}
+
+PK_API int pk_pbd_rollout_backward(pk_ctx* c, const float* xbar, const float* vbar, float* grad_x0, float* grad_v0,
+                                   pk_stream stream)
+{
+    return pbd_backward_entry<float>(c, xbar, vbar, grad_x0, grad_v0, stream, "pk_pbd_rollout_backward");
+}
+
+PK_API int pk_pbd_rollout_f64(pk_ctx* c, double* x, double* v, int n, const pk_pbf_params* p, int steps,
+                              int checkpoint_every, pk_stream stream)
+{
+    return pbd_rollout_entry<double>(c, x, v, n, p, steps, checkpoint_every, stream, "pk_pbd_rollout_f64");
+}
+
+PK_API int pk_pbd_rollout_backward_f64(pk_ctx* c, const double* xbar, const double* vbar, double* grad_x0,
+                                       double* grad_v0, pk_stream stream)
+{
+    return pbd_backward_entry<double>(c, xbar, vbar, grad_x0, grad_v0, stream, "pk_pbd_rollout_backward_f64");
 }
 
 // ======================================================================

@@ -137,6 +137,7 @@ struct pk_ctx {
     int* pd_in_off = nullptr;   // their CSR offsets (n + 1)
     int2* pd_in = nullptr;      // (source particle, bond slot) of every incoming bond
     // projection workspaces (float, double) and the parameters of the last rollout
+    void* pbd_roll = nullptr;   // differentiable DensityPBD rollout (pk_pbd_adj.cu)
     void* pd_work32 = nullptr;
     void* pd_work64 = nullptr;
     float pd_horizon_last = 0.f, pd_mu_last = 0.f, pd_lambda_last = 0.f;

@@ -26,6 +26,8 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap,
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,
                    float* x, float* v, float* rho_out, cudaStream_t st, float viscosity = 0.f,
                    int vis_iterations = 0);
+int pbd_replay_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt, float4* ys,
+                     float* x, float* v, cudaStream_t st);
 int viscosity_generic(pk_ctx* c, const float* x, float* v, int n, const int* index, const int* elements, int cap,
                       long long total, float vis, float h, int iterations, float dt, cudaStream_t st);
 int pbd_generic_solve(pk_ctx* c, float* x, float* v, int n, const int* index, const int* elements,
@@ -80,6 +82,15 @@ int pd_backward_f32(pk_ctx* c, const float* xbar, const float* vbar, float* gx, 
 int pd_backward_f64(pk_ctx* c, const double* xbar, const double* vbar, double* gx, double* gv, double* gbulk,
                     cudaStream_t st);
 void pd_work_release(pk_ctx* c);
+
+// pk_pbd_adj.cu: differentiable DensityPBD rollouts (float or double state);
+// -1 when memory runs out, -2 (backward) when no matching rollout is recorded.
+template <class T>
+int pbd_rollout_impl(pk_ctx* c, T* x, T* v, int n, const pk_pbf_params* p, int steps, int every, int row_cap,
+                     cudaStream_t st);
+template <class T>
+int pbd_backward_impl(pk_ctx* c, const T* xbar, const T* vbar, T* gx, T* gv, cudaStream_t st);
+void pbd_roll_release(pk_ctx* c);
 
 // pk_pd.cu
 int pd_rest_shape(pk_ctx* c, const float* x, int n, const int* index, const int* elements,

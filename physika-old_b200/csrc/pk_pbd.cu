@@ -538,6 +538,27 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     return launches;
 }
 
+// pbd_fast_solve without viscosity, keeping every Jacobi iterate for a
+// reverse pass: ys[0..n) holds y_0 (the integrated positions, as sorted by
+// the frame's build), iteration t reads ys[t n ..) and writes ys[(t+1) n ..)
+// with the same kernels and arithmetic, so the iterates are those of the
+// fused frame bit for bit.  Then x, v in caller order as k_finish writes them.
+int pbd_replay_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt, float4* ys,
+                     float* x, float* v, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    const int pb = c->tune.pass_block;
+    const unsigned nb1 = (unsigned)((n + 255) / 256), nbp = (unsigned)((n + pb - 1) / pb);
+    const PassK pk = pass_k(k, mass);
+    for (int it = 0; it < iterations; ++it) {
+        by_block<LaunchDensity>(pb, nbp, st, ys + (size_t)it * n, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                nullptr);
+        by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, ys + (size_t)(it + 1) * n);
+    }
+    k_finish<<<nb1, 256, 0, st>>>(ys + (size_t)iterations * n, ys, c->vs, c->rho, c->perm, n, dt, x, v, nullptr);
+    return 2 * iterations + 1;
+}
+
 int gather_state(pk_ctx* c, const float* x, const float* v, int n, cudaStream_t st)
 {
     if (n <= 0) return 0;

@@ -1,12 +1,19 @@
-"""torch.autograd.Function over the peridynamics rollout of the C ABI.
+"""torch.autograd.Function over the differentiable rollouts of the C ABI.
 
 PdRollout.apply(x0, v0, bulk, ctx, settings) runs `steps` ElasticityModule
 steps (integration + projection) on the sm_100a library and returns x_T; its
 backward calls the hand-written adjoint (pk_pd_rollout_backward), which
 replays the rollout from checkpoints and returns dL/dx0, dL/dv0 and dL/dbulk.
+The context must have been initialised with pd_init on the rest shape; bond
+breaking is not differentiable and is off.
+
+PbdRollout.apply(x0, v0, ctx, params, steps, checkpoint_every) runs `steps`
+DensityPBD frames (list, integration, Jacobi solve, velocity update; no
+boundary, no viscosity) and returns (x_T, v_T); its backward calls
+pk_pbd_rollout_backward and returns dL/dx0 and dL/dv0.
+
 float32 and float64 tensors are supported (the float64 path is the reference
-for gradient checks).  The context must have been initialised with pd_init on
-the rest shape; bond breaking is not differentiable and is off.
+for gradient checks).
 """
 from dataclasses import dataclass
 
@@ -51,3 +58,23 @@ class PdRollout(torch.autograd.Function):
 def pd_rollout(x0, v0, bulk, pk_ctx, settings):
     """x_T of the rollout; differentiable in x0, v0 and bulk."""
     return PdRollout.apply(x0, v0, bulk, pk_ctx, settings)
+
+
+class PbdRollout(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, x0, v0, pk_ctx, params, steps, checkpoint_every):
+        x = x0.detach().clone().contiguous()
+        v = v0.detach().clone().contiguous()
+        pk_ctx.pbd_rollout(x, v, params, steps, checkpoint_every)
+        fctx.pk_ctx = pk_ctx
+        return x, v
+
+    @staticmethod
+    def backward(fctx, gx_t, gv_t):
+        gx, gv = fctx.pk_ctx.pbd_rollout_backward(gx_t.contiguous(), gv_t.contiguous())
+        return gx, gv, None, None, None, None
+
+
+def pbd_rollout(x0, v0, pk_ctx, params, steps, checkpoint_every=20):
+    """(x_T, v_T) of the DensityPBD rollout; differentiable in x0 and v0."""
+    return PbdRollout.apply(x0, v0, pk_ctx, params, steps, checkpoint_every)

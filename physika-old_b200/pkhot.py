@@ -25,6 +25,7 @@ EXPORTED = [
     "pk_pd_rotate_rest_shape", "pk_pd_apply_yielding", "pk_pd_reconstruct_rest_shape", "pk_pd_fracture",
     "pk_pd_get_yield", "pk_pd_get_bulk", "pk_pd_rest_layout",
     "pk_pd_rollout", "pk_pd_rollout_backward", "pk_pd_rollout_f64", "pk_pd_rollout_backward_f64",
+    "pk_pbd_rollout", "pk_pbd_rollout_backward", "pk_pbd_rollout_f64", "pk_pbd_rollout_backward_f64",
     "pk_noalloc_max_particles", "pk_pbd_solve_noalloc",
 ]
 
@@ -124,6 +125,10 @@ def load():
         "pk_pd_rollout_f64": ([P, P, P, P, I, ctypes.POINTER(ctypes.c_double * 3), ctypes.POINTER(PdParams),
                                I, I, P], I),
         "pk_pd_rollout_backward_f64": ([P, P, P, P, P, P, P], I),
+        "pk_pbd_rollout": ([P, P, P, I, ctypes.POINTER(PbfParams), I, I, P], I),
+        "pk_pbd_rollout_backward": ([P, P, P, P, P, P], I),
+        "pk_pbd_rollout_f64": ([P, P, P, I, ctypes.POINTER(PbfParams), I, I, P], I),
+        "pk_pbd_rollout_backward_f64": ([P, P, P, P, P, P], I),
         "pk_noalloc_max_particles": ([], I),
         "pk_pbd_solve_noalloc": ([P, P, I, P, P, I, LL, ctypes.POINTER(PbdParams), P, P], I),
     }
@@ -380,6 +385,24 @@ class Context:
         fn = self.L.pk_pd_rollout_backward_f64 if xbar.dtype == torch.float64 else self.L.pk_pd_rollout_backward
         self._check(fn(self.h, _ptr(xbar), _ptr(vbar), _ptr(gx), _ptr(gv), _ptr(gb), _stream()))
         return gx, gv, gb
+
+    def pbd_rollout(self, x, v, params, steps=1, checkpoint_every=0):
+        """`steps` DensityPBD frames (no boundary, no viscosity) in place, keeping
+        a checkpoint every `checkpoint_every` steps for pbd_rollout_backward.
+        x, v float32 or float64 (the double run of the same method)."""
+        import torch
+        fn = self.L.pk_pbd_rollout_f64 if x.dtype == torch.float64 else self.L.pk_pbd_rollout
+        self._check(fn(self.h, _ptr(x), _ptr(v), x.shape[0], ctypes.byref(params), int(steps),
+                       int(checkpoint_every), _stream()))
+
+    def pbd_rollout_backward(self, xbar, vbar=None):
+        """(dL/dx0, dL/dv0) of the last rollout of xbar's precision, given dL/dx_T
+        (and dL/dv_T)."""
+        import torch
+        gx, gv = torch.empty_like(xbar), torch.empty_like(xbar)
+        fn = self.L.pk_pbd_rollout_backward_f64 if xbar.dtype == torch.float64 else self.L.pk_pbd_rollout_backward
+        self._check(fn(self.h, _ptr(xbar), _ptr(vbar), _ptr(gx), _ptr(gv), _stream()))
+        return gx, gv
 
     # ---- autotuning of the frame kernels
     def autotune(self, enable=True):
