@@ -46,12 +46,19 @@ WORKLOAD = ("dam_break_2m: 128^3 jittered lattice, spacing 0.0025, radius 0.0062
             "5 Jacobi iterations, dt 5e-4, box 2x1x1")
 
 
-def pass_bytes(kind, kbar, kunion):
-    """Algorithmic bytes per particle of one launch of a solver pass."""
-    if kind == "density":  # read x_i, the N(i) row, write lambda
+def stage_bytes(kind, kbar, kunion):
+    """Algorithmic bytes per particle of one launch of a stage of the frame;
+    the stages add up to pbd_bytes_per_particle_step."""
+    if kind == "sort":  # boundary (read x, v; write x, v) + integrate (read x, v; write x, v, x_old)
+        return 48.0 + 60.0
+    if kind == "build":  # neighbour build: read x, write the list and its count
         return 12.0 + 4.0 * kbar + 4.0
-    if kind == "disp":  # read x_i, lambda_i, the row, write x_i'
+    if kind == "density":  # pass A: read x_i, the N(i) row, write lambda
+        return 12.0 + 4.0 * kbar + 4.0
+    if kind == "disp":  # pass B: read x_i, lambda_i, the row, write x_i'
         return 12.0 + 4.0 + 4.0 * kunion + 12.0
+    if kind == "finish":  # velocity update (read x, x_old, v; write v) + density out
+        return 48.0 + 4.0
     raise ValueError(kind)
 
 
@@ -202,11 +209,14 @@ BATCHED_WORKLOAD = ("256 independent dam-break scenes, particle counts log-unifo
 
 
 def measure_batched(local, steps, warmup, barrier, max_over_ranks, rank, world):
-    """The batched frame (one pk_pbf_step_batched for all scenes, also replayed
-    as a CUDA graph) against per-scene plain frames (one pk_pbf_step per scene),
-    same scenes, same GPU, device time with CUDA events.  With several ranks the
-    scenes are partitioned (largest first to the least-loaded rank) and each
-    rank steps its share; times are the max over ranks, values the whole job."""
+    """The batched frame (one pk_pbf_step_batched for all scenes, eager and
+    replayed as a graph recorded by pk_graph_capture) against per-scene plain
+    frames (one pk_pbf_step per scene per frame, issued from the C++ host loop
+    pkf_pbf_frames_per_scene), same scenes, same GPU, device time with CUDA
+    events.  With several ranks the scenes are partitioned (largest first to
+    the least-loaded rank) and each rank steps its share; times are the max
+    over ranks, values the whole job."""
+    import ctypes
     import torch
     import pkhot
     from sharding import partition_scenes, subset
@@ -227,7 +237,6 @@ def measure_batched(local, steps, warmup, barrier, max_over_ranks, rank, world):
     x = torch.from_numpy(b.x.copy()).to(dev)
     v = torch.zeros_like(x)
     off = torch.from_numpy(b.offsets.astype(np.int32)).to(dev)
-    stream = torch.cuda.current_stream()
 
     def timed(fn, k):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -243,51 +252,50 @@ def measure_batched(local, steps, warmup, barrier, max_over_ranks, rank, world):
         ctx.pbf_step_batched(x, v, off, prm)
     ctx.check_status()
     launches = ctx.launch_count()
+    kbar, kunion, _ = ctx.row_stats()
     ms_eager = timed(lambda: ctx.pbf_step_batched(x, v, off, prm), steps)
-    graph_ms, graph_note, g = None, None, None
-    try:
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            ctx.pbf_step_batched(x, v, off, prm)
-        g.replay()
-    except Exception as exc:  # the eager number still stands
-        g, graph_note = None, f"capture failed: {exc}"
-    # every rank times the graph, or none does (the timing has collectives)
-    if max_over_ranks(0.0 if g is not None else 1.0) == 0.0:
-        graph_ms = timed(g.replay, steps)
-    elif graph_note is None:
-        graph_note = "capture failed on another rank"
-    g = None
+    ctx.graph_capture(x, v, prm, off)
+    ms_graph = timed(ctx.graph_launch, steps)
+    ctx.graph_release()
     ctx.check_status()
-    lo, hi = b.offsets[:-1], b.offsets[1:]
-    views = [(x[a:c], v[a:c]) for a, c in zip(lo, hi)]
+    # per-scene plain frames, issued from C++
+    fw = ctypes.CDLL(os.path.join(os.path.dirname(pkhot.LIB_PATH), "libpkframework.so"))
+    fw.pkf_pbf_frames_per_scene.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.POINTER(pkhot.PbfParams), ctypes.c_int,
+                                            ctypes.c_void_p]
+    offs_host = (ctypes.c_int * len(b.offsets))(*[int(q) for q in b.offsets])
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
     def plain_frame():
-        for xs, vs in views:
-            ctx.pbf_step(xs, vs, prm)
+        rc = fw.pkf_pbf_frames_per_scene(ctx.h, x.data_ptr(), v.data_ptr(), offs_host, len(b.scenes),
+                                         ctypes.byref(prm), 1, stream)
+        if rc != 0:
+            raise RuntimeError(f"pkf_pbf_frames_per_scene: {rc}")
 
     plain_frame()
     ctx.check_status()
     ms_plain = timed(plain_frame, max(2, min(steps, 5)))
     ctx.check_status()
     ctx.close()
-    del stream
 
     def entry(ms):
         return {"value": n_all / (ms / 1e3), "unit": UNIT, "ms_per_step": ms}
 
-    out = {"workload": BATCHED_WORKLOAD, "scenes": len(b_all.scenes), "particles": n_all,
-           "scenes_per_rank": "largest-first greedy partition" if world > 1 else "all",
-           "batched_eager": entry(ms_eager), "plain_per_scene": entry(ms_plain),
-           "launches_per_frame": {"batched": launches, "plain": launches * len(b.scenes)},
-           "speedup_vs_plain": ms_plain / ms_eager}
-    if graph_ms is not None:
-        out["batched_graph"] = entry(graph_ms)
-        out["speedup_vs_plain"] = ms_plain / min(graph_ms, ms_eager)
-    else:
-        out["batched_graph"] = None
-        out["graph_note"] = graph_note
-    return out
+    peak, peak_kind = peaks()
+    best = min(ms_eager, ms_graph)
+    # sum over scenes of B_PBD(N_s, K_s) plus the scene-offset table; the
+    # bytes are linear in K, so the whole job's mean K gives the sum
+    frame_bytes = world * (n * pbd_bytes_per_particle_step(kbar, sc0.iterations) + 16.0 * len(b.scenes))
+    return {"workload": BATCHED_WORKLOAD, "scenes": len(b_all.scenes), "particles": n_all,
+            "scenes_per_rank": "largest-first greedy partition" if world > 1 else "all",
+            "batched_eager": entry(ms_eager), "batched_graph": entry(ms_graph),
+            "plain_per_scene": entry(ms_plain),
+            "plain_per_scene_issue": "pkf_pbf_frames_per_scene: C++ host loop, one pk_pbf_step per scene",
+            "launches_per_frame": {"batched": launches, "plain": launches * len(b.scenes)},
+            "speedup_vs_plain": ms_plain / best,
+            "roofline": {"bound": "hbm", "bytes_per_frame": frame_bytes, "kbar": kbar,
+                         "achieved": frame_bytes / (best / 1e3) / 1e9 / world, "peak": peak, "unit": "GB/s",
+                         "frac": frame_bytes / (best / 1e3) / 1e9 / world / peak, "peak_source": peak_kind}}
 
 
 ADJOINT_WORKLOAD = ("differentiable rollout: 64x32x32 = 65,536-particle peridynamics block, spacing 0.004, "
@@ -422,7 +430,7 @@ def measure_elastoplastic(local, steps, warmup, barrier):
             "steps": steps, "yielding_particles_last_frame": yielding}
 
 
-def measure_adjoint(local, fd_coords=16):
+def measure_adjoint(local, fd_coords=64):
     """cfg4: float rollout with checkpoints, its reverse pass, and a check of
     the double-precision adjoint against central differences of double rollouts."""
     import torch
@@ -516,6 +524,55 @@ def measure_adjoint(local, fd_coords=16):
             "fp32_vs_fp64_gradient_rel": rel32}
 
 
+PBD_ADJOINT_WORKLOAD = ("differentiable dam-break rollout: 64x32x32 = 65,536-particle fluid block with the 32k "
+                        "dam break's parameters (spacing 0.005, +-0.1 spacing jitter, radius 0.0125, cap 60, "
+                        "5 DensityPBD iterations, dt 1e-3, gravity), off the walls (no boundary), initial "
+                        "velocities N(0, 0.05^2) (PCG64 seed 1), 200 frames, checkpoint every 20; loss = mean "
+                        "|x_T - x_target|^2 against a run from half the initial velocities")
+
+
+def measure_pbd_adjoint(local):
+    """The DensityPBD rollout with checkpoints and its reverse pass
+    (pk_pbd_rollout / pk_pbd_rollout_backward), device time; the gradient
+    checks against central differences are the tests'."""
+    import torch
+    import pkhot
+
+    dev = torch.device("cuda", local)
+    base = scenes.dam_break_small(seed=0, n_side=1)
+    x0 = torch.from_numpy(scenes.lattice(64, 32, 32, base.spacing, 0.1, 0, origin=(0.3, 0.3, 0.3))).to(dev)
+    v0 = torch.from_numpy(np.random.Generator(np.random.PCG64(1)).normal(0.0, 0.05, tuple(x0.shape))
+                          .astype(np.float32)).to(dev)
+    n = x0.shape[0]
+    prm = pkhot.pbf_params(pkhot.nq_params(base.radius, base.lo, base.hi, base.cap),
+                           pkhot.pbd_params(base.radius, base.spacing, base.rest_density, base.iterations,
+                                            base.dt), base.gravity, boundary=False)
+    steps, every = 200, 20
+    ctx = pkhot.Context(local)
+    xt, vt = x0.clone(), v0 * 0.5
+    ctx.pbd_rollout(xt, vt, prm, steps, 0)
+    x, v = x0.clone(), v0.clone()
+    ctx.pbd_rollout(x, v, prm, steps, every)  # warm-up: workspaces
+    ctx.pbd_rollout_backward(2.0 * (x - xt) / n)
+    x, v = x0.clone(), v0.clone()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    ctx.pbd_rollout(x, v, prm, steps, every)
+    ev[1].record()
+    gx, gv = ctx.pbd_rollout_backward(2.0 * (x - xt) / n)
+    ev[2].record()
+    torch.cuda.synchronize()
+    ctx.check_status()
+    fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    loss = float(((x - xt) ** 2).sum(1).mean())
+    ctx.close()
+    return {"workload": PBD_ADJOINT_WORKLOAD, "particles": n, "steps": steps, "checkpoint_every": every,
+            "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "forward_particle_steps_per_s": n * steps / (fwd / 1e3), "loss": loss,
+            "gradient_norm": {"x0": float(gx.norm()), "v0": float(gv.norm())}}
+
+
 def run_pk(args):
     import torch
     import torch.distributed as dist
@@ -605,12 +662,15 @@ def run_pk(args):
     ctx.check_status()
 
     peak, peak_kind = peaks()
-    # dominant kernel class over the timed region
-    dom = max(("density", "disp"), key=lambda k: prof[k][0])
-    dom_ms, dom_launches = prof[dom]
+    # stages of the frame: the neighbour build is the sweep + selection
+    # ("select") and the row emission ("emit")
+    stages = {"sort": prof["sort"], "build": (prof["select"][0] + prof["emit"][0], prof["select"][1]),
+              "density": prof["density"], "disp": prof["disp"], "finish": prof["finish"]}
+    total_ms = sum(t for t, _ in stages.values())
+    dom = max(stages, key=lambda k: stages[k][0])
+    dom_ms, dom_launches = stages[dom]
     traffic = load_traffic().get(dom)
-    # rows of the displacement pass hold N(i) plus the mirror entries (kunion)
-    per_launch_bytes = n * pass_bytes(dom, kbar, kunion)
+    per_launch_bytes = n * stage_bytes(dom, kbar, kunion)
     achieved = per_launch_bytes / (dom_ms / dom_launches / 1e3) / 1e9
     step_bytes = pbd_bytes_per_particle_step(kbar, sc.iterations)
     step_frac = value / world * step_bytes / (peak * 1e9)
@@ -624,9 +684,14 @@ def run_pk(args):
                    "parallelism": "replicas" if world > 1 else "single",
                    "tuned": {"pass_threads_per_block": tuned_pass, "build_particles_per_pass": tuned_build},
                    "l2": "working set > L2 (neighbour rows alone are > 1 GB); no flush"},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes},
+        "roofline": {"bound": "hbm", "kernel": dom, "share": dom_ms / total_ms, "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "frame": {"bytes_per_particle_step": step_bytes,
+                               "achieved": value / world * step_bytes / 1e9, "frac": step_frac}},
+        "stage_roofline": {k: {"share": t / total_ms,
+                               "frac": n * stage_bytes(k, kbar, kunion) / (t / nl / 1e3) / 1e9 / peak}
+                           for k, (t, nl) in stages.items()},
         "step_roofline": {"bytes_per_particle_step": step_bytes, "frac": step_frac,
                           "peak_source": peak_kind},
         "kernel_ms": {k: {"total_ms": prof[k][0], "launches": prof[k][1]} for k in prof},
@@ -663,6 +728,7 @@ def run_pk(args):
         line["elastoplastic"] = measure_elastoplastic(local, max(3, min(args.steps, 10)), 3, barrier)
     if not args.no_adjoint:
         line["adjoint"] = measure_adjoint(local)
+        line["adjoint_pbd"] = measure_pbd_adjoint(local)
     if rank == 0 and world == 1 and not args.no_cpu:
         cv, cores, cn = time_cpu(steps=2, warmup=1)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port",

@@ -201,4 +201,25 @@ __attribute__((visibility("default"))) int pkf_elastoplastic_run(const float* x,
     }
 }
 
+// Independent fluid scenes stepped the way the reference steps them: every
+// scene its own frame, each frame its own launches (one pk_pbf_step per scene
+// per frame, issued from this host loop).  x, v: device arrays of all scenes'
+// particles concatenated; offsets: host array of nscenes + 1 particle offsets.
+// The baseline against which pk_pbf_step_batched (one frame for all scenes)
+// is measured.  Returns the first non-zero pk status, else 0.
+__attribute__((visibility("default"))) int pkf_pbf_frames_per_scene(pk_ctx* ctx, float* x, float* v,
+                                                                    const int* offsets, int nscenes,
+                                                                    const pk_pbf_params* p, int frames,
+                                                                    pk_stream stream)
+{
+    if (!ctx || !x || !v || !offsets || nscenes < 1 || !p || frames < 0) return PK_ERR_ARG;
+    for (int f = 0; f < frames; ++f)
+        for (int s = 0; s < nscenes; ++s) {
+            const int a = offsets[s], n = offsets[s + 1] - a;
+            const int rc = pk_pbf_step(ctx, x + 3LL * a, v + 3LL * a, n, p, nullptr, stream);
+            if (rc != PK_OK) return rc;
+        }
+    return PK_OK;
+}
+
 }  // extern "C"
