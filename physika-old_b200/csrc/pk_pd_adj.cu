@@ -127,12 +127,9 @@ __device__ __forceinline__ void unit_fast(V3<R>& u)
 // takes bonds sub, sub + kPdG, ... and the group's partial sums are combined
 // with xor shuffles in a fixed order (deterministic, so a replayed rollout
 // repeats the forward bit for bit).
-// The bond walks load the next bond's flag, neighbour and rest position (and
-// the gather the next incoming slot) while the current one is used: 9.12 ->
-// 8.35 ms per elastic-bar step, the same results.
-#ifndef PK_PD_PF
-#define PK_PD_PF 1
-#endif
+// The deformation walk loads the next bond's flag, neighbour and rest
+// position (and the gather the next incoming slot) while the current one is
+// used: 9.12 -> 8.35 ms per elastic-bar step, the same results.
 constexpr int kPdG = 8;
 constexpr int kPdBlock = 128;
 constexpr unsigned kPdAll = 0xffffffffu;
@@ -164,9 +161,13 @@ __device__ __forceinline__ PdLane pd_lane(int n)
 // p = (x_j - x_i)/h, q = e wt / h, e = rest_j - rest_i, and the identity when
 // det F < -0.001.  Called by all lanes of i's group; every lane gets F, tw
 // and whether the identity was taken.
+// With `stash`, the lane's first kPdStash bonds are kept in shared memory
+// (rest vector e and the neighbour, stored as ~j for a dead bond) for a
+// second walk over them.
+constexpr int kPdStash = 10;  // bonds per lane: cap 80 over 8 lanes
 template <class R, class RX>
 __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, int sub, R F[3][3], float& tw_out,
-                               bool& ident)
+                               bool& ident, float4 (*stash)[kPdBlock] = nullptr)
 {
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
@@ -175,7 +176,6 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, int sub, R 
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) F[a][b] = 0;
     float tw = 0.f;
-#if PK_PD_PF
     // the next bond's flag, neighbour and rest position are loaded one bond ahead
     bool al_n = false;
     int j_n = 0;
@@ -189,19 +189,13 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, int sub, R 
         r2_n = B.rpos[3 * at + 2];
     };
     if (sub < m) load(sub);
-    for (int e = sub; e < m; e += kPdG) {
+    for (int e = sub, k = 0; e < m; e += kPdG, ++k) {
         const bool al = al_n;
         const int j = j_n;
         const float e0 = r0_n - ri0, e1 = r1_n - ri1, e2 = r2_n - ri2;
         if (e + kPdG < m) load(e + kPdG);
+        if (stash && k < kPdStash) stash[k][threadIdx.x] = make_float4(e0, e1, e2, __int_as_float(al ? j : ~j));
         if (!al) continue;
-#else
-    for (int e = sub; e < m; e += kPdG) {
-        const long long at = pd_at(B.index, B.cap, i, e);
-        if (!B.alive[at]) continue;
-        const int j = B.ridx[at];
-        const float e0 = B.rpos[3 * at] - ri0, e1 = B.rpos[3 * at + 1] - ri1, e2 = B.rpos[3 * at + 2] - ri2;
-#endif
         const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
         if (r > kEpsilon) {
             const float wt = corr_w_f(r, B.inv_h);
@@ -374,18 +368,23 @@ __global__ void __launch_bounds__(kPdBlock)
 // k_pd_FP computes F_i and every outgoing t_ij of particle i, keeps the sum
 // in own[i] and each t_ij in its bond slot (0 for a dead or too-short bond),
 // and k_pd_gather sums -t over the incoming slots: no neighbour F is
-// gathered and no bond is evaluated twice.
+// gathered and no bond is evaluated twice.  k_pd_FP's two walks over a
+// particle's bonds (F, then the terms) read the rest shape once: the first
+// keeps each lane's bonds in shared memory for the second.
 template <class R>
 __global__ void __launch_bounds__(kPdBlock)
     k_pd_FP(PdBonds B, const R* __restrict__ x, const R* __restrict__ bulk, R* __restrict__ Fout,
             float* __restrict__ twout, R* __restrict__ own, R* __restrict__ tslot)
 {
+    // the first walk's bonds, read again by the second from shared memory
+    // instead of from the rest shape in DRAM
+    __shared__ float4 stash[kPdStash][kPdBlock];
     const PdLane L = pd_lane(B.n);
     const int i = L.i;
     R Fi[3][3];
     float tw;
     bool ident;
-    pd_deformation(B, x, i, L.sub, Fi, tw, ident);
+    pd_deformation(B, x, i, L.sub, Fi, tw, ident, stash);
     if (L.valid && L.sub == 0) {
         for (int a = 0; a < 3; ++a)
             for (int b = 0; b < 3; ++b) Fout[9LL * i + 3 * a + b] = Fi[a][b];
@@ -396,33 +395,27 @@ __global__ void __launch_bounds__(kPdBlock)
     const V3<R> ci = ld3(x, i);
     const int m = pd_size(B.index, B.cap, B.total, B.n, i);
     V3<R> acc{0, 0, 0};
-#if PK_PD_PF
-    bool al_n = false;
-    int j_n = 0;
-    float r0_n = 0.f, r1_n = 0.f, r2_n = 0.f;
-    auto load = [&](int ee) {
-        const long long at = pd_at(B.index, B.cap, i, ee);
-        al_n = B.alive[at];
-        j_n = B.ridx[at];
-        r0_n = B.rpos[3 * at];
-        r1_n = B.rpos[3 * at + 1];
-        r2_n = B.rpos[3 * at + 2];
-    };
-    if (L.sub < m) load(L.sub);
-#endif
-    for (int e = L.sub; e < m; e += kPdG) {
+    for (int e = L.sub, k = 0; e < m; e += kPdG, ++k) {
         const long long at = pd_at(B.index, B.cap, i, e);
         V3<R> t{0, 0, 0};
-#if PK_PD_PF
-        const bool al = al_n;
-        const int j = j_n;
-        const float e0 = ri0 - r0_n, e1 = ri1 - r1_n, e2 = ri2 - r2_n;
-        if (e + kPdG < m) load(e + kPdG);
-#else
-        const bool al = B.alive[at];
-        const int j = B.ridx[at];
-        const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
-#endif
+        bool al;
+        int j;
+        float e0, e1, e2;
+        if (k < kPdStash) {
+            const float4 q = stash[k][threadIdx.x];
+            const int jv = __float_as_int(q.w);
+            al = jv >= 0;
+            j = al ? jv : ~jv;
+            e0 = -q.x;  // the stash holds rest_j - rest_i
+            e1 = -q.y;
+            e2 = -q.z;
+        } else {
+            al = B.alive[at];
+            j = B.ridx[at];
+            e0 = ri0 - B.rpos[3 * at];
+            e1 = ri1 - B.rpos[3 * at + 1];
+            e2 = ri2 - B.rpos[3 * at + 2];
+        }
         const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
         if (al && r > 0.01f * B.h) {
             const V3<R> xj = ld3(x, j);
@@ -466,7 +459,6 @@ __global__ void __launch_bounds__(kPdBlock)
     const PdLane L = pd_lane(B.n);
     const int i = L.i;
     V3<R> in{0, 0, 0};
-#if PK_PD_PF
     const int t1 = B.in_off[i + 1];
     int t = B.in_off[i] + L.sub;
     int slot_n = t < t1 ? B.in_list[t].y : 0;  // the next incoming slot, one bond ahead
@@ -477,14 +469,6 @@ __global__ void __launch_bounds__(kPdBlock)
         in.y += g[1];
         in.z += g[2];
     }
-#else
-    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
-        const R* g = tslot + 4 * (long long)B.in_list[t].y;
-        in.x += g[0];
-        in.y += g[1];
-        in.z += g[2];
-    }
-#endif
     in.x = gsum(in.x);
     in.y = gsum(in.y);
     in.z = gsum(in.z);
