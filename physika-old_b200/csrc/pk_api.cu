@@ -55,7 +55,7 @@ int ensure_particles(pk_ctx* c, int n)
               regrow(c->xs_pre, m) && regrow(c->xs0, m) && regrow(c->xa, m) && regrow(c->xb, m) &&
               regrow(c->vs, m) && regrow(c->vv, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
               regrow(c->tau, m) && regrow(c->tau_hint, m) && regrow(c->hcnt, m) && regrow(c->items, m + 1) &&
-              regrow(c->nitems, 1);
+              regrow(c->nitems, 1) && regrow(c->ovf, m) && regrow(c->ovf_list, m);
     if (!ok) {
         c->cap_n = 0;
         return fail(c, PK_ERR_NOMEM, "device allocation of particle scratch failed");
@@ -77,6 +77,36 @@ int ensure_rows(pk_ctx* c, long long m)
     }
     c->cap_rows = m;
     return PK_OK;
+}
+
+// The spill pool: 8 entries per particle, or what the last synchronised build
+// found it needed (and a quarter more).
+constexpr long long kPoolPerParticle = 8;
+
+int ensure_pool(pk_ctx* c, int n)
+{
+    long long want = std::max<long long>((long long)n * kPoolPerParticle, 4096);
+    if (c->pool_need > 0) want = std::max(want, c->pool_need + c->pool_need / 4);
+    want = std::min<long long>((want + 3) & ~3LL, (1LL << 31) - 4);
+    if (want <= c->pool_cap) return PK_OK;
+    if (!regrow(c->hpool, (size_t)want) || !regrow(c->rpool, (size_t)want)) {
+        c->pool_cap = 0;
+        return fail(c, PK_ERR_NOMEM, "device allocation of the spill pool failed");
+    }
+    c->pool_cap = want;
+    return PK_OK;
+}
+
+// Entries the last build handed out of the spill pool (also past its
+// capacity); stream-ordered read, so the caller has synchronised.
+long long spill_used(pk_ctx* c, cudaStream_t st)
+{
+    unsigned long long used = 0;
+    if (cudaMemcpyAsync(&used, c->spill, sizeof(used), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return -1;
+    if ((long long)used > c->pool_cap) c->pool_need = std::max(c->pool_need, (long long)used);
+    return (long long)used;
 }
 
 int ensure_keys(pk_ctx* c, long long nk, int n)
@@ -112,14 +142,15 @@ int ensure_generic(pk_ctx* c, int n)
     return PK_OK;
 }
 
-// Rows first hold every hit of a particle (before the capped compaction), so
-// they are sized to the per-particle hit bound (512); a dynamic list may ask
-// for less with max_neighbors.
+// Entries per particle kept in the main hit and solver rows: 128, or 2 cap
+// for a larger cap, or a dynamic list's max_neighbors (a multiple of 4).
+// Longer rows continue in the spill pool.
 int row_capacity(const pk_nq_params* p)
 {
-    if (p->cap > 0) return pk::kMaxHits;
-    int m = p->max_neighbors > 0 ? p->max_neighbors : pk::kMaxHits;
-    return std::min(m, pk::kMaxHits);
+    int m = pk::kRowCapMin;
+    if (p->cap > 0) m = std::max(m, 2 * p->cap);
+    if (p->cap <= 0 && p->max_neighbors > 0) m = std::max(m, p->max_neighbors);
+    return std::min((m + 3) & ~3, pk::kRowCapMax);
 }
 
 int check_nq(pk_ctx* c, const pk_nq_params* p)
@@ -128,8 +159,8 @@ int check_nq(pk_ctx* c, const pk_nq_params* p)
     if (!(p->radius > 0.0f) || !std::isfinite(p->radius))
         return fail(c, PK_ERR_ARG, "radius must be positive and finite");
     if (p->cap < 0 || p->cap > 448) return fail(c, PK_ERR_ARG, "cap must be in [0, 448]");
-    if (p->max_neighbors < 0 || p->max_neighbors > pk::kMaxHits)
-        return fail(c, PK_ERR_ARG, "max_neighbors must be in [0, 512]");
+    if (p->max_neighbors < 0 || p->max_neighbors > pk::kRowCapMax)
+        return fail(c, PK_ERR_ARG, "max_neighbors must be in [0, 4096]");
     for (int a = 0; a < 3; ++a)
         if (!(p->hi[a] > p->lo[a])) return fail(c, PK_ERR_ARG, "bounding box must have hi > lo");
     pk::Grid g = pk::make_grid(p->radius, p->lo, p->hi);
@@ -229,7 +260,11 @@ PK_API int pk_ctx_create(pk_ctx** out, int device)
     pk_ctx* c = new pk_ctx();
     c->device = device;
     if (cudaMalloc((void**)&c->d_err, sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
+        cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&c->spill, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(c->spill, 0, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+        if (c->d_err) cudaFree(c->d_err);
+        if (c->spill) cudaFree(c->spill);
         delete c;
         return PK_ERR_NOMEM;
     }
@@ -251,7 +286,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau, c->tau_hint, c->pl_y1, c->pl_y2, c->pl_i1, c->pl_yield,
                     c->pl_invF, c->pl_sizes, c->pl_off, c->pl_rest_idx2, c->pl_rest_pos2,
                     c->hcnt, c->items, c->nitems,
-                    c->rows, c->hits, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
+                    c->rows, c->hits, c->hpool, c->rpool, c->ovf, c->ovf_list, c->spill, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
                     c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v, c->pd_ktw, c->pl_mk};
@@ -286,7 +321,13 @@ PK_API int pk_ctx_status(pk_ctx* c, pk_stream stream)
             snprintf(msg, sizeof msg, "a particle id outside [0, n) was given in pins or a neighbour list (flags 0x%x)", bits);
             return fail(c, PK_ERR_ARG, msg);
         }
-        snprintf(msg, sizeof msg, "capacity exceeded on the device (flags 0x%x: 1=row, 2=hits>512, 4=list)", bits);
+        const long long used = spill_used(c, (cudaStream_t)stream);
+        if (bits & pk::kErrHitOverflow)
+            snprintf(msg, sizeof msg,
+                     "the spill pool of long neighbour rows ran out (flags 0x%x; %lld entries needed, %lld held; "
+                     "the next build grows it)", bits, used, c->pool_cap);
+        else
+            snprintf(msg, sizeof msg, "capacity exceeded on the device (flags 0x%x: 1=row, 4=list)", bits);
         return fail(c, PK_ERR_CAPACITY, msg);
     }
     return PK_OK;
@@ -379,12 +420,22 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
     c->nq_h = p->radius;
     c->exported_index = index;
     c->exported_elements = elements;
-    int launches = pk::sort_particles(c, const_cast<float*>(x), nullptr, nullptr, n, g, false, nullptr,
-                                      0.f, 0.f, 0.f, false, nullptr, st);
-    launches += pk::build_rows(c, n, g, p->radius, p->cap, row_cap, index, elements,
-                               elements ? elements_capacity : 0, st);
+    // rows longer than the capacity go to the spill pool; a pool too small for
+    // this build is grown to what the build asked for and the build repeated
+    int launches = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if ((rc = ensure_pool(c, n))) return rc;
+        launches = pk::sort_particles(c, const_cast<float*>(x), nullptr, nullptr, n, g, false, nullptr, 0.f, 0.f,
+                                      0.f, false, nullptr, st);
+        launches += pk::build_rows(c, n, g, p->radius, p->cap, row_cap, index, elements,
+                                   elements ? elements_capacity : 0, st);
+        if ((rc = check_launch(c, "pk_nq_build"))) return rc;
+        const long long used = spill_used(c, st);
+        if (used < 0) return cuda_fail(c, cudaGetLastError(), "pk_nq_build");
+        if (used <= c->pool_cap) break;
+        cudaMemset(c->d_err, 0, sizeof(int));  // the repeated build replaces this one
+    }
     c->launches = launches;
-    if ((rc = check_launch(c, "pk_nq_build"))) return rc;
     c->nq_valid = true;
     if (total) {
         if (p->cap > 0) {
@@ -745,7 +796,7 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     }
     const int row_cap = row_capacity(&p->nq);
     if ((rc = ensure_particles(c, n)) || (rc = ensure_keys(c, g.nkeys + 1, n)) ||
-        (rc = ensure_rows(c, pk::row_slots(n, row_cap))))
+        (rc = ensure_rows(c, pk::row_slots(n, row_cap))) || (rc = ensure_pool(c, n)))
         return rc;
     pk::SdfView sv{};
     if (p->boundary) sv = pk::sdf_view(c);
@@ -836,9 +887,9 @@ PK_API int pk_pbf_step_batched(pk_ctx* c, float* x, float* v, const int* scene_o
 
 namespace {
 
-// Hits per particle the rollout's rows hold (its frames keep every step's
-// rows for the reverse pass, so they are sized to what fluids reach rather
-// than to the 512-hit bound of pk_pbf_step).
+// Hits per particle the rollout's rows hold.  Its frames keep every step's
+// rows for the reverse pass, so a longer row is a capacity error there
+// instead of continuing in the spill pool as in pk_pbf_step.
 constexpr int kRollRowCap = 128;
 
 int pbd_roll_check(pk_ctx* c, int n, const pk_pbf_params* p, int steps, int every, const void* x,

@@ -39,10 +39,22 @@ struct pk_ctx {
     uint2* tau = nullptr;
     unsigned* tau_hint = nullptr;  // caller order: d2 bits of the last frame's tau (selection pivot)
 
-    // ---- rows (capacity cap_rows entries)
+    // ---- rows (capacity cap_rows entries: row_cap per particle)
     long long cap_rows = 0;
     int* rows = nullptr;      // solver rows: sorted index | flag bits
     uint2* hits = nullptr;    // hit rows: (sorted index, d2 bits), candidate order
+    // Entries of a particle past row_cap (hits and solver row alike) go to the
+    // spill pool: ovf[s] is the particle's segment, holding round4(count -
+    // row_cap) entries of each array.  spill[0] counts the entries handed out
+    // in the last build (also past pool_cap: the size the next build grows the
+    // pool to), spill[1] the particles listed in ovf_list.
+    long long pool_cap = 0;
+    long long pool_need = 0;  // entries the last synchronised build asked for
+    uint2* hpool = nullptr;
+    int* rpool = nullptr;
+    int* ovf = nullptr;       // per sorted particle (valid where its count > row_cap)
+    int* ovf_list = nullptr;  // sorted particles with a spill segment
+    unsigned long long* spill = nullptr;  // 2 device counters
 
     // ---- dense cell table (capacity cap_keys entries + 2)
     long long cap_keys = 0;

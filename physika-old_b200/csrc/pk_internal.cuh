@@ -24,7 +24,13 @@ constexpr float kEpsilon = 1e-6f;  // cuda_utilities.h:30
 constexpr int kRowFlagA = 1 << 31;
 constexpr int kRowFlagB = 1 << 30;
 constexpr int kRowIndexMask = (1 << 30) - 1;
-constexpr int kMaxHits = 512;  // per-particle hit buffer of the list build
+// Per-particle row capacity of the hit rows and solver rows held in the main
+// arrays (kRowCapMin, or 2 cap for a larger cap, or a dynamic list's
+// max_neighbors).  A particle with more hits keeps the rest of its hit row and
+// of its solver row in the spill pool, so no count of particles inside one
+// radius is too large for a list.
+constexpr int kRowCapMin = 128;
+constexpr int kRowCapMax = 4096;
 
 // Solver rows are interleaved by blocks of 32 sorted particles and quads of
 // entries: entries 4q .. 4q+3 of particle s are 16 contiguous bytes at
@@ -43,9 +49,22 @@ __host__ __device__ inline long long row_slots(long long n, int row_cap)
     return ((n + 31) & ~31LL) * 4LL * row_quads(row_cap);
 }
 
+// Row entry e of sorted particle s (e < its row length): the main array up
+// to the row capacity, then the particle's spill segment.
+struct RowView {
+    const int* rows;
+    const int* rpool;
+    const int* ovf;
+    int rc;
+    __device__ __forceinline__ int at(int s, int e) const
+    {
+        return e < rc ? rows[row_slot(s, e, rc)] : rpool[ovf[s] + (e - rc)];
+    }
+};
+
 // Error bits latched in Ctx::d_err.
-constexpr int kErrRowOverflow = 1;
-constexpr int kErrHitOverflow = 2;
+constexpr int kErrRowOverflow = 1;  // a row over the capacity of a build without spill
+constexpr int kErrHitOverflow = 2;  // the spill pool ran out (it grows for the next build)
 constexpr int kErrPublicOverflow = 4;
 constexpr int kErrBadIndex = 8;  // a particle id outside [0, n) (pins)
 

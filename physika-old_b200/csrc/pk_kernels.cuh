@@ -18,9 +18,12 @@ int sort_particles(pk_ctx* c, float* x, float* v, const float* f, int n, const G
                    bool integrate, const float grav[3], cudaStream_t st);
 
 // pk_nbr.cu: the cap-nearest selection and the row emission over the sorted
-// particles.  pub_index/pub_elements may be null.  Returns kernels launched.
+// particles.  pub_index/pub_elements may be null.  With spill, rows longer
+// than row_cap continue in the context's spill pool; without, they are a
+// capacity error.  Returns kernels launched.
 int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap,
-               int* pub_index, int* pub_elements, long long pub_capacity, cudaStream_t st);
+               int* pub_index, int* pub_elements, long long pub_capacity, cudaStream_t st,
+               bool spill = true);
 
 // pk_pbd.cu
 int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations, float dt,

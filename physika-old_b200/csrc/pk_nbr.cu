@@ -27,10 +27,13 @@
 //     sqrt_rn is monotone, so the key order agrees with the reference's
 //     distance order except among hits at exactly equal distance, which the
 //     reference orders by arrival.
-//   k_emit (8 lanes per particle): re-reads the hit row, marks a = key <= tau_i
-//     (j in N(i)) and b = key' <= tau_j (i in N(j)), compacts in place with
-//     a-entries first, then b-only entries, and writes the public NeighborList
-//     in caller ids (fixed: index = count; dynamic: CSR).
+//   k_spill (particles with more hits than the row capacity): the same sweep
+//     for one particle, keeping the hits past the capacity in the particle's
+//     segment of the spill pool, so a row of any length is in candidate order.
+//   k_emit (one thread per particle): re-reads the hit row a quad at a time,
+//     marks a = key <= tau_i (j in N(i)) and b = key' <= tau_j (i in N(j)),
+//     writes the solver row with a-entries first, then b-only entries, and the
+//     public NeighborList in caller ids (fixed: index = count; dynamic: CSR).
 // Distances use the explicit roundings of exact_norm3's squared sum, so every
 // d < h decision and every ordering is bit-identical for (i, j) and (j, i)
 // and matches the CPU restatement.
@@ -78,11 +81,36 @@ struct BuildArgs {
     int n, row_cap;
     float T;            // d2 threshold of d < h
     uint2* hits;        // hit rows: (sorted index, d2 bits), candidate order
-    int* hcnt;          // hits per particle (sorted order)
+    int* hcnt;          // hits per particle (sorted order), past the row capacity too
     int* count_c;       // hits per particle in caller order (dynamic public list), or null
     const int* perm;
     int* err;
+    // spill pool (pool_cap 0: none, a row past the capacity is an error)
+    long long pool_cap;
+    unsigned long long* spill;  // [0] entries handed out, [1] particles listed
+    int* ovf;
+    int* ovf_list;
+    uint2* hpool;
 };
+
+// Entries past the row capacity: a segment of round4(count - row_cap) entries
+// of the spill pool, and the particle listed for k_spill.
+__device__ __forceinline__ void claim_spill(const BuildArgs& A, int s, int count)
+{
+    if (A.pool_cap <= 0) {
+        atomicOr(A.err, kErrRowOverflow);
+        return;
+    }
+    const unsigned long long need = (unsigned long long)((count - A.row_cap + 3) & ~3);
+    const unsigned long long off = atomicAdd(A.spill, need);
+    if (off + need <= (unsigned long long)A.pool_cap) {
+        A.ovf[s] = (int)off;
+        A.ovf_list[atomicAdd(A.spill + 1, 1ull)] = s;
+    } else {
+        A.ovf[s] = -1;
+        atomicOr(A.err, kErrHitOverflow);
+    }
+}
 
 // Particles of one pass, held in registers by every lane: 8 by default, 4 or
 // 16 when the context's autotuner measured that faster (the hit rows are the
@@ -111,6 +139,37 @@ __device__ __forceinline__ float4 fetch_cand(const float4* __restrict__ xs, cons
         if (r + step < 27 && S.roff[r + step] <= g) r += step;
     t = S.rbeg[r] + (g - S.roff[r]);
     return __ldg(xs + t);
+}
+
+// The 27 neighbour ranges of sorted particle s's cell into S (lane o < 27
+// owns offset o; the reference's visiting order), packed in that order;
+// returns the candidate count.  Called by a whole warp.
+__device__ __forceinline__ int sweep_ranges(const BuildArgs& A, SweepSmem& S, int s, int lane)
+{
+    const float4 x0 = A.xs[s];
+    const int3 c = cell3(A.g, x0.x, x0.y, x0.z);
+    const int base = scene_key_base(A.g, __ldg(A.perm + s));
+    int beg = 0, len = 0;
+    if (lane < 27) {
+        const int key = cell_key(A.g, c.x + kOffset27[lane][0], c.y + kOffset27[lane][1], c.z + kOffset27[lane][2]);
+        if (key >= 0) {
+            beg = __ldg(A.start + base + key);
+            len = __ldg(A.start + base + key + 1) - beg;
+        }
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    __syncwarp();
+    S.rbeg[lane] = beg;
+    S.roff[lane] = incl - len;
+    const int total = __shfl_sync(kFull, incl, 31);
+    if (lane == 31) S.roff[32] = total;
+    __syncwarp();
+    return total;
 }
 
 // One pass of the sweep: kPB particles in registers against every candidate
@@ -168,31 +227,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, build_min_blocks<KPB>()) k_b
     const int gw = blockIdx.x * kBuildWarps + w, nw = gridDim.x * kBuildWarps;
     for (int item = gw; item < nitems; item += nw) {
         const int2 rng = A.items[item];
-        const float4 x0 = A.xs[rng.x];
-        const int3 c = cell3(A.g, x0.x, x0.y, x0.z);
-        const int base = scene_key_base(A.g, __ldg(A.perm + rng.x));
-        // the 27 neighbour ranges in one round: lane o < 27 owns offset o
-        int beg = 0, len = 0;
-        if (lane < 27) {
-            const int key = cell_key(A.g, c.x + kOffset27[lane][0], c.y + kOffset27[lane][1],
-                                     c.z + kOffset27[lane][2]);
-            if (key >= 0) {
-                beg = __ldg(A.start + base + key);
-                len = __ldg(A.start + base + key + 1) - beg;
-            }
-        }
-        int incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += y;
-        }
-        __syncwarp();
-        S.rbeg[lane] = beg;
-        S.roff[lane] = incl - len;
-        const int total = __shfl_sync(kFull, incl, 31);
-        if (lane == 31) S.roff[32] = total;
-        __syncwarp();
+        const int total = sweep_ranges(A, S, rng.x, lane);
         for (int p0 = rng.x; p0 < rng.y; p0 += KPB) {
             const int m = min(KPB, rng.y - p0);
             float px[KPB], py[KPB], pz[KPB];
@@ -217,11 +252,41 @@ __global__ void __launch_bounds__(kBuildWarps * 32, build_min_blocks<KPB>()) k_b
             for (int p = 0; p < KPB; ++p) {
                 if (lane == p && p < m) {
                     const int s = p0 + p;
-                    A.hcnt[s] = min(cnt[p], A.row_cap);
+                    A.hcnt[s] = cnt[p];
                     if (A.count_c) A.count_c[A.perm[s]] = cnt[p];
-                    if (cnt[p] > A.row_cap) atomicOr(A.err, kErrRowOverflow);
+                    if (cnt[p] > A.row_cap) claim_spill(A, s, cnt[p]);
                 }
             }
+        }
+    }
+}
+
+// Hits past the row capacity: one warp per listed particle repeats the
+// particle's sweep (same ranges, same candidate order) and writes the hits
+// numbered row_cap and up to its spill segment.
+__global__ void __launch_bounds__(kBuildWarps * 32) k_spill(BuildArgs A)
+{
+    extern __shared__ int smem_i[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    SweepSmem& S = reinterpret_cast<SweepSmem*>(smem_i)[w];
+    const long long listed = (long long)A.spill[1];
+    const long long gw = (long long)blockIdx.x * kBuildWarps + w, nw = (long long)gridDim.x * kBuildWarps;
+    for (long long item = gw; item < listed; item += nw) {
+        const int s = A.ovf_list[item];
+        const int off = A.ovf[s];
+        const int total = sweep_ranges(A, S, s, lane);
+        const float4 xi = A.xs[s];
+        int cnt = 0;
+        for (int c0 = 0; c0 < total; c0 += 32) {
+            int t;
+            const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
+            const float d2 = exact_d2(xi, cx);
+            const bool hit = d2 < A.T;
+            const unsigned b = __ballot_sync(kFull, hit);
+            const int pos = cnt + __popc(b & lt);
+            if (hit && pos >= A.row_cap) A.hpool[off + (pos - A.row_cap)] = make_uint2((unsigned)t, __float_as_uint(d2));
+            cnt += __popc(b);
         }
     }
 }
@@ -229,6 +294,19 @@ __global__ void __launch_bounds__(kBuildWarps * 32, build_min_blocks<KPB>()) k_b
 // ---- tau_i: the cap-th smallest key (d2, sorted index) of each hit row.
 constexpr int kSelWarps = 8;
 constexpr int kSelRegChunks = 4;  // rows of up to 128 hits are held in registers
+
+// Hit e of one particle's row: the main array up to the row capacity, then
+// the particle's spill segment.
+struct HitRow {
+    const uint2* row;
+    const uint2* pool;  // the particle's spill segment (null when none)
+    int rc;
+    __device__ __forceinline__ uint2 at(int e) const
+    {
+        if (e < rc) return __ldg(row + e);
+        return pool ? __ldg(pool + (e - rc)) : make_uint2(0u, 0xffffffffu);
+    }
+};
 
 struct SelSmem {
     int hist[kBins];
@@ -251,8 +329,8 @@ __device__ __forceinline__ int sel_bin(unsigned db, float lo, float scale)
 // index.  Src supplies the row: chunk k of 32 entries (lanes past c hold
 // d2 bits 0xffffffff, outside every interval).
 template <class Src>
-__device__ __forceinline__ uint2 select_rank(const Src& src, int nch, const uint2* __restrict__ row, int c, int rr, float T,
-                             SelSmem& S, int lane, unsigned lt)
+__device__ __forceinline__ uint2 select_rank(const Src& src, int nch, const HitRow& row, int c, int rr, float T,
+                                             SelSmem& S, int lane, unsigned lt)
 {
     unsigned plo = 0u, phi = __float_as_uint(T);  // [0, T]: every hit
     float lo = 0.f, scale = (float)kBins / T;
@@ -314,11 +392,11 @@ __device__ __forceinline__ uint2 select_rank(const Src& src, int nch, const uint
     } else {
         // more than 32 hits at one d2 value: the rr-th smallest index
         for (int e = lane; e < c; e += 32) {
-            const uint2 v = __ldg(row + e);
+            const uint2 v = row.at(e);
             if (v.y != plo) continue;
             int rank = 0;
             for (int u = 0; u < c; ++u) {
-                const uint2 o = __ldg(row + u);
+                const uint2 o = row.at(u);
                 rank += (o.y == plo && o.x < v.x) ? 1 : 0;
             }
             if (rank == rr) mine = make_uint2(v.y, v.x);
@@ -344,12 +422,12 @@ struct RegSrc {
 };
 // Row chunks from memory (longer rows).
 struct MemSrc {
-    const uint2* row;
+    HitRow row;
     int c, lane;
     __device__ __forceinline__ uint2 operator()(int k) const
     {
         const int e = k * 32 + lane;
-        return e < c ? __ldg(row + e) : make_uint2(0u, 0xffffffffu);
+        return e < c ? row.at(e) : make_uint2(0u, 0xffffffffu);
     }
 };
 
@@ -438,7 +516,8 @@ __device__ __forceinline__ uint2 select_pivot(const uint2 (&h)[4], int c, int ca
 #endif
 __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
     k_select(const uint2* __restrict__ hits, const int* __restrict__ hcnt, int n, int cap, int row_cap,
-             float T, uint2* __restrict__ tau, const int* __restrict__ perm, unsigned* __restrict__ tau_hint)
+             float T, uint2* __restrict__ tau, const int* __restrict__ perm, unsigned* __restrict__ tau_hint,
+             const uint2* __restrict__ hpool, const int* __restrict__ ovf)
 {
     __shared__ SelSmem sm[kSelWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -470,7 +549,12 @@ __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
             const int q = __ffs(need) - 1;
             need &= need - 1;
             const int c = __shfl_sync(kFull, c_l, q);
-            const uint2* row = hits + (base + q) * row_cap;
+            const long long sq = base + q;
+            HitRow row{hits + sq * row_cap, nullptr, row_cap};
+            if (c > row_cap) {
+                const int o = __ldg(ovf + sq);
+                row.pool = o >= 0 ? hpool + o : nullptr;
+            }
             uint2 h[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) h[k] = hn[k];
@@ -496,116 +580,154 @@ __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
     }
 }
 
-// Solver rows from the hit rows: G lanes per particle.
-constexpr int kEmitG = 8;
-constexpr int kStash = 128;  // b-only entries kept per group before appending
-// Chunks of kEmitG entries whose loads are issued together, and resident
-// blocks per SM asked of the register allocator: 2 chunks at 8 blocks (32
-// registers) measured fastest at 2M, ahead of 1, 3 or 4 chunks at 4-6 blocks.
-#ifndef PK_EMIT_U
-#define PK_EMIT_U 2
-#endif
-#ifndef PK_EMIT_MINB
-#define PK_EMIT_MINB 8
-#endif
-constexpr int kEmitU = PK_EMIT_U;
+// Solver rows from the hit rows, one thread per particle.  The thread reads
+// its hit row two quads (8 hits, 64 contiguous bytes) at a time, gathers
+// tau_j of those hits (L2-resident), marks a and b, and writes its solver
+// row a quad (16 bytes) at a time into the interleaved layout: a-entries in
+// hit order, then the b-only entries, which wait in shared memory (kEmitStash
+// per thread; a second walk over the row picks up any beyond).  Rows longer
+// than the capacity continue in the particle's spill segment.
+constexpr int kEmitBlock = 256;
+constexpr int kEmitStash = 16;
 
-__global__ void __launch_bounds__(256, PK_EMIT_MINB)
-    k_emit(const int* __restrict__ hcnt, const uint2* __restrict__ hits, const uint2* __restrict__ tau,
-           const int* __restrict__ perm, int n, int cap, int row_cap, int* __restrict__ rows,
-           int2* __restrict__ rcnt, int* __restrict__ pub_index, int* __restrict__ pub_elements,
-           long long pub_capacity, const int* __restrict__ offs, int* __restrict__ err)
+struct EmitArgs {
+    const int* hcnt;
+    const uint2* hits;
+    const uint2* hpool;  // null: no spill pool
+    const int* ovf;
+    const uint2* tau;
+    const int* perm;
+    int n, cap, rc;
+    int* rows;
+    int* rpool;
+    int2* rcnt;
+    int* pub_index;
+    int* pub_elements;
+    long long pub_capacity;
+    const int* offs;
+    int* err;
+};
+
+// One particle's solver row, written in order a quad at a time.
+struct RowOut {
+    int4* q0;   // quad 0 of the particle's interleaved row (its quads are 32 apart)
+    int* pool;  // the particle's spill segment, or null
+    int rc, len;
+    int4 pend;
+    bool over;
+    __device__ __forceinline__ void flush(int q)
+    {
+        if (4 * q < rc)
+            q0[32LL * q] = pend;
+        else if (pool)
+            *reinterpret_cast<int4*>(pool + (4 * q - rc)) = pend;
+        else
+            over = true;
+    }
+    __device__ __forceinline__ void put(int v)
+    {
+        const int k = len & 3;
+        if (k == 0) pend.x = v;
+        if (k == 1) pend.y = v;
+        if (k == 2) pend.z = v;
+        if (k == 3) pend.w = v;
+        ++len;
+        if ((len & 3) == 0) flush((len >> 2) - 1);
+    }
+    __device__ __forceinline__ void finish()
+    {
+        if (len & 3) flush(len >> 2);
+    }
+};
+
+__global__ void __launch_bounds__(kEmitBlock) k_emit(EmitArgs A)
 {
-    __shared__ int s_b[256 / kEmitG][kStash];  // b-only entries of each group
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = gid / kEmitG, sub = gid % kEmitG, grp = threadIdx.x / kEmitG;
-    const int lane = threadIdx.x & 31;
-    const unsigned gmask = ((1u << kEmitG) - 1u) << (lane & ~(kEmitG - 1));
-    const unsigned lt_g = ((1u << lane) - 1u) & gmask;
-    const bool valid = s < n;
-    const bool capped = cap > 0;
-    int cnt = 0, ps = 0;
-    uint2 ti = make_uint2(0x7f800000u, 0x7fffffffu);
-    long long pbase = 0;
-    const bool pub = pub_elements != nullptr;
-    if (valid) {
-        cnt = hcnt[s];
-        if (capped) ti = tau[s];
-        ps = perm[s];
-        if (pub) pbase = capped ? (long long)ps * cap : (long long)offs[ps];
-    }
-    const int so = valid ? s : 0;
-    const uint2* hrow = hits + (long long)so * row_cap;
-    // every lane of the warp iterates to the longest row of the warp's groups
-    int cmax = cnt;
+    __shared__ int stash[kEmitStash][kEmitBlock];
+    const int s = blockIdx.x * kEmitBlock + threadIdx.x;
+    if (s >= A.n) return;  // no warp-wide operation follows
+    const bool capped = A.cap > 0;
+    const int c = A.hcnt[s];
+    const uint2 ti = capped ? A.tau[s] : make_uint2(0x7f800000u, 0x7fffffffu);
+    const int ps = A.perm[s];
+    const bool pub = A.pub_elements != nullptr;
+    const long long pbase = pub ? (capped ? (long long)ps * A.cap : (long long)A.offs[ps]) : 0;
+    const uint2* hrow = A.hits + (long long)s * A.rc;
+    const int o = (c > A.rc && A.hpool) ? A.ovf[s] : -1;
+    const uint2* hseg = o >= 0 ? A.hpool + o : nullptr;
+    // hits past the capacity are lost only when the pool ran out (latched by the build)
+    const int cm = (c > A.rc && !hseg) ? A.rc : c;
+    RowOut out;
+    out.q0 = reinterpret_cast<int4*>(A.rows) + (long long)(s >> 5) * row_quads(A.rc) * 32 + (s & 31);
+    out.pool = o >= 0 ? A.rpool + o : nullptr;
+    out.rc = A.rc;
+    out.len = 0;
+    out.pend = make_int4(0, 0, 0, 0);
+    out.over = false;
+    bool pub_over = false;
+    int nB = 0;
+    for (int e0 = 0; e0 < cm; e0 += 8) {
+        uint2 h[8], tj[8];
 #pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
-    int nA = 0, nB = 0;
-    bool over = false;
-    // kEmitU chunks per round: their hit loads, then their tau_j gathers, are
-    // all in flight before the first ballot (the chunks are then decided and
-    // written in order, as one chunk at a time would)
-    for (int e0 = 0; e0 < cmax; e0 += kEmitG * kEmitU) {
-        uint2 h[kEmitU], tj[kEmitU];
-#pragma unroll
-        for (int u = 0; u < kEmitU; ++u) {
-            const int e = e0 + u * kEmitG + sub;
-            h[u] = (valid && e < cnt) ? __ldg(hrow + e) : make_uint2(0u, 0u);
-        }
-#pragma unroll
-        for (int u = 0; u < kEmitU; ++u) {
-            const int e = e0 + u * kEmitG + sub;
-            tj[u] = (capped && valid && e < cnt) ? __ldg(tau + h[u].x) : make_uint2(0u, 0u);
-        }
-#pragma unroll
-        for (int u = 0; u < kEmitU; ++u) {
-            if (e0 + u * kEmitG >= cmax) break;  // warp-uniform: cmax is the warp's maximum
-            const int e = e0 + u * kEmitG + sub;
-            bool fa = false, fb = false;
-            const int t = (int)h[u].x;
-            if (valid && e < cnt) {
-                if (capped) {
-                    const float d2 = __uint_as_float(h[u].y);
-                    fa = key_le(d2, t, ti);
-                    fb = key_le(d2, s, tj[u]);
-                } else {
-                    fa = fb = true;
-                }
+        for (int u = 0; u < 2; ++u) {
+            const int e = e0 + 4 * u;  // a quad lies wholly in the main row or in the segment
+            uint4 a = make_uint4(0u, 0u, 0u, 0u), b = a;
+            if (e < cm) {
+                const uint2* src = e < A.rc ? hrow + e : hseg + (e - A.rc);
+                a = __ldg(reinterpret_cast<const uint4*>(src));
+                b = __ldg(reinterpret_cast<const uint4*>(src + 2));
             }
-            const unsigned ba = __ballot_sync(kFull, fa) & gmask;
-            const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
+            h[4 * u] = make_uint2(a.x, a.y);
+            h[4 * u + 1] = make_uint2(a.z, a.w);
+            h[4 * u + 2] = make_uint2(b.x, b.y);
+            h[4 * u + 3] = make_uint2(b.z, b.w);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) tj[k] = (capped && e0 + k < cm) ? __ldg(A.tau + h[k].x) : make_uint2(0u, 0u);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (e0 + k >= cm) break;
+            const int t = (int)h[k].x;
+            bool fa = true, fb = true;
+            if (capped) {
+                const float d2 = __uint_as_float(h[k].y);
+                fa = key_le(d2, t, ti);
+                fb = key_le(d2, s, tj[k]);
+            }
             if (fa) {
-                const int q = nA + __popc(ba & lt_g);
-                rows[row_slot(so, q, row_cap)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
                 if (pub) {
-                    const long long o = pbase + q;
-                    if (capped ? (q < cap) : (o < pub_capacity))
-                        pub_elements[o] = __ldg(perm + t);
+                    const long long po = pbase + out.len;
+                    if (capped ? (out.len < A.cap) : (po < A.pub_capacity))
+                        A.pub_elements[po] = __ldg(A.perm + t);
                     else
-                        over = true;
+                        pub_over = true;
                 }
+                out.put(t | kRowFlagA | (fb ? kRowFlagB : 0));
+            } else if (fb) {
+                if (nB < kEmitStash) stash[nB][threadIdx.x] = t | kRowFlagB;
+                ++nB;
             }
-            if (fb && !fa) {
-                const int q = nB + __popc(bb & lt_g);
-                if (q < kStash)
-                    s_b[grp][q] = t | kRowFlagB;
-                else
-                    over = true;
-            }
-            nA += __popc(ba);
-            nB += __popc(bb);
         }
     }
-    __syncwarp();
-    if (valid) {
-        const int nBw = min(nB, kStash);
-        for (int e = sub; e < nBw; e += kEmitG) rows[row_slot(so, nA + e, row_cap)] = s_b[grp][e];
-        if (sub == 0) {
-            rcnt[s] = make_int2(nA, nA + nBw);
-            if (pub_index != nullptr) pub_index[ps] = capped ? min(nA, cap) : offs[ps];
+    const int nA = out.len;
+    const int nS = min(nB, kEmitStash);
+    for (int k = 0; k < nS; ++k) out.put(stash[k][threadIdx.x]);
+    if (nB > kEmitStash) {
+        // the b-only entries past the stash, in hit order (capped lists only)
+        int seen = 0;
+        for (int e = 0; e < cm; ++e) {
+            const uint2 hh = e < A.rc ? __ldg(hrow + e) : __ldg(hseg + (e - A.rc));
+            const float d2 = __uint_as_float(hh.y);
+            const int t = (int)hh.x;
+            if (key_le(d2, t, ti) || !key_le(d2, s, __ldg(A.tau + t))) continue;
+            if (seen++ >= kEmitStash) out.put(t | kRowFlagB);
         }
     }
-    if (__any_sync(kFull, over) && lane == 0) atomicOr(err, kErrPublicOverflow);
+    out.finish();
+    // a row cut short (no spill segment) reports what it holds; the error is latched
+    A.rcnt[s] = out.over ? make_int2(min(nA, A.rc), min(out.len, A.rc)) : make_int2(nA, out.len);
+    if (A.pub_index != nullptr) A.pub_index[ps] = capped ? min(nA, A.cap) : A.offs[ps];
+    if (out.over) atomicOr(A.err, kErrRowOverflow);
+    if (pub_over) atomicOr(A.err, kErrPublicOverflow);
 }
 
 // Smallest float T with sqrt_rn(T) >= h: for every float d2, sqrt_rn(d2) < h
@@ -619,7 +741,7 @@ static float radius_threshold(float h)
 }
 
 int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, int* pub_index,
-               int* pub_elements, long long pub_capacity, cudaStream_t st)
+               int* pub_elements, long long pub_capacity, cudaStream_t st, bool spill)
 {
     if (n <= 0) return 0;
     int dev = 0, sms = 0, per_sm = 0;
@@ -652,8 +774,14 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     A.count_c = dyn_pub ? c->count_c : nullptr;
     A.perm = c->perm;
     A.err = c->d_err;
+    A.pool_cap = spill ? c->pool_cap : 0;
+    A.spill = c->spill;
+    A.ovf = c->ovf;
+    A.ovf_list = c->ovf_list;
+    A.hpool = c->hpool;
     const int blocks = std::min((n + kBuildWarps - 1) / kBuildWarps, sms * per_sm);
     prof_begin(c, PK_PROF_SELECT, st);
+    cudaMemsetAsync(c->spill, 0, 2 * sizeof(unsigned long long), st);
     if (c->tune.on) cudaEventRecord(c->tune.ev[0], st);
     if (pbn == 8)
         k_build<8><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
@@ -663,10 +791,16 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
         k_build<kPB><<<blocks, kBuildWarps * 32, kBuildSmem, st>>>(A);
     if (c->tune.on) cudaEventRecord(c->tune.ev[1], st);
     ++launches;
+    const uint2* hpool = A.pool_cap > 0 ? c->hpool : nullptr;
+    if (hpool) {
+        // the hits past the row capacity (an empty launch when no row is that long)
+        k_spill<<<sms * 2, kBuildWarps * 32, kBuildSmem, st>>>(A);
+        ++launches;
+    }
     if (capped) {
         const int sb = (int)std::min<long long>(((long long)n + 32 * kSelWarps - 1) / (32 * kSelWarps), (long long)sms * 8);
         k_select<<<sb, kSelWarps * 32, 0, st>>>(c->hits, c->hcnt, n, cap, row_cap, A.T, c->tau, c->perm,
-                                                c->tau_hint);
+                                                c->tau_hint, hpool, hpool ? c->ovf : nullptr);
         ++launches;
     }
     if (dyn_pub) {
@@ -675,9 +809,25 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     }
     prof_end(c, PK_PROF_SELECT, st);
     prof_begin(c, PK_PROF_EMIT, st);
-    const unsigned ne = (unsigned)(((long long)n * kEmitG + 255) / 256);
-    k_emit<<<ne, 256, 0, st>>>(c->hcnt, c->hits, c->tau, c->perm, n, cap, row_cap, c->rows, c->rcnt,
-                               pub_index, pub_elements, pub_capacity, c->offs, c->d_err);
+    EmitArgs E;
+    E.hcnt = c->hcnt;
+    E.hits = c->hits;
+    E.hpool = hpool;
+    E.ovf = c->ovf;
+    E.tau = c->tau;
+    E.perm = c->perm;
+    E.n = n;
+    E.cap = cap;
+    E.rc = row_cap;
+    E.rows = c->rows;
+    E.rpool = c->rpool;
+    E.rcnt = c->rcnt;
+    E.pub_index = pub_index;
+    E.pub_elements = pub_elements;
+    E.pub_capacity = pub_capacity;
+    E.offs = c->offs;
+    E.err = c->d_err;
+    k_emit<<<(unsigned)((n + kEmitBlock - 1) / kEmitBlock), kEmitBlock, 0, st>>>(E);
     prof_end(c, PK_PROF_EMIT, st);
     return launches + 1;
 }

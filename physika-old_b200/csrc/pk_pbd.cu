@@ -49,6 +49,15 @@ constexpr int kPassBlock = PK_PASS_BLOCK;  // threads per block of the Jacobi pa
 // pass and outgrow L2).
 __device__ __forceinline__ int4 row_quad(const int4* p) { return __ldcs(p); }
 
+// Entries of a solver row past the row capacity: the particle's spill
+// segment (rows that long exist only where more particles than the capacity
+// sit inside one radius).
+struct Tail {
+    const int* rpool;
+    const int* ovf;
+    __device__ __forceinline__ int entry(int s, int k) const { return __ldg(rpool + __ldg(ovf + s) + k); }
+};
+
 // Pass A: rho_i and lambda_i over N(i), one thread per particle walking its
 // interleaved row.  Writes xl[s] = (x_i, lambda_i) so pass B gathers a
 // neighbour's position and lambda in one 16-byte load.  sum |grad_j|^2 is taken
@@ -56,14 +65,28 @@ __device__ __forceinline__ int4 row_quad(const int4* p) { return __ldcs(p); }
 __global__ void __launch_bounds__(kPassBlock)
     k_pass_density(const float4* __restrict__ xs, const int* __restrict__ rows,
                    const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
-                   float4* __restrict__ xl, float* __restrict__ rho_out)
+                   float4* __restrict__ xl, float* __restrict__ rho_out, Tail tl)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float4 xi = xs[s];
-    const int na = rcnt[s].x;
+    const int na_all = rcnt[s].x, na = min(na_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     float rho = 0.f, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    auto pair = [&](int v) {
+        const float4 xj = __ldg(xs + (v & kRowIndexMask));
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        float d2, ir, dd;
+        pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
+        const float dd2 = dd * dd;
+        rho = fmaf(k_.cwm, dd2 * dd, rho);
+        const float g = d2 > kEps2 ? k_.cg * dd2 : 0.0f;
+        const float gi = g * ir;
+        gx = fmaf(gi, dx, gx);
+        gy = fmaf(gi, dy, gy);
+        gz = fmaf(gi, dz, gz);
+        sg = fmaf(g, g, sg);
+    };
     const int nq = (na + 3) >> 2;
     int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
     for (int q = 0; q < nq; ++q) {
@@ -73,21 +96,10 @@ __global__ void __launch_bounds__(kPassBlock)
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (4 * q + k >= na) break;
-            const int j = ent[k] & kRowIndexMask;
-            const float4 xj = __ldg(xs + j);
-            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            float d2, ir, dd;
-            pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
-            const float dd2 = dd * dd;
-            rho = fmaf(k_.cwm, dd2 * dd, rho);
-            const float g = d2 > kEps2 ? k_.cg * dd2 : 0.0f;
-            const float gi = g * ir;
-            gx = fmaf(gi, dx, gx);
-            gy = fmaf(gi, dy, gy);
-            gz = fmaf(gi, dz, gz);
-            sg = fmaf(g, g, sg);
+            pair(ent[k]);
         }
     }
+    for (int e = na; e < na_all; ++e) pair(tl.entry(s, e - na));
     float l = sg + (gx * gx + gy * gy + gz * gz);
     l = -(rho - 1000.0f) / (l + 0.1f);  // rest density hard-coded (DensityPBD.cu:87)
     xl[s] = make_float4(xi.x, xi.y, xi.z, l > 0.0f ? 0.0f : l);
@@ -99,14 +111,25 @@ __global__ void __launch_bounds__(kPassBlock)
 // bits; one thread per particle.
 __global__ void __launch_bounds__(kPassBlock)
     k_pass_disp(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
-                int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
+                int row_cap, int n, PassK k_, float4* __restrict__ xs_out, Tail tl)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float4 xi = xl[s];
-    const int nu = rcnt[s].y;
+    const int nu_all = rcnt[s].y, nu = min(nu_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     float ax = 0.f, ay = 0.f, az = 0.f;
+    auto pair = [&](int v) {
+        const float mult = (float)__popc((unsigned)v >> 30);
+        const float4 xj = __ldg(xl + (v & kRowIndexMask));
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        float d2, ir, dd;
+        pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
+        const float c = d2 > kEps2 ? mult * (xi.w + xj.w) * (k_.c10g * (dd * dd)) * ir : 0.0f;
+        ax = fmaf(c, dx, ax);
+        ay = fmaf(c, dy, ay);
+        az = fmaf(c, dz, az);
+    };
     const int nq = (nu + 3) >> 2;
     int4 nxt = nq > 0 ? row_quad(rq) : make_int4(0, 0, 0, 0);
     for (int q = 0; q < nq; ++q) {
@@ -116,19 +139,10 @@ __global__ void __launch_bounds__(kPassBlock)
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (4 * q + k >= nu) break;
-            const int v = ent[k];
-            const int j = v & kRowIndexMask;
-            const float mult = (float)__popc((unsigned)v >> 30);
-            const float4 xj = __ldg(xl + j);
-            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            float d2, ir, dd;
-            pair_geom(dx, dy, dz, k_.inv_h, d2, ir, dd);
-            const float c = d2 > kEps2 ? mult * (xi.w + xj.w) * (k_.c10g * (dd * dd)) * ir : 0.0f;
-            ax = fmaf(c, dx, ax);
-            ay = fmaf(c, dy, ay);
-            az = fmaf(c, dz, az);
+            pair(ent[k]);
         }
     }
+    for (int e = nu; e < nu_all; ++e) pair(tl.entry(s, e - nu));
     xs_out[s] = make_float4(xi.x + ax, xi.y + ay, xi.z + az, 0.f);
 }
 
@@ -213,12 +227,12 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
     k_pass_density2(const float4* __restrict__ xs, const int* __restrict__ rows,
                     const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
-                    float4* __restrict__ xl, float* __restrict__ rho_out)
+                    float4* __restrict__ xl, float* __restrict__ rho_out, Tail tl)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float4 xi = xs[s];
-    const int na = rcnt[s].x;
+    const int na_all = rcnt[s].x, na = min(na_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     DensAcc a{};
     const int nfull = na >> 2, nq = (na + 3) >> 2;
@@ -242,6 +256,7 @@ __global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
         for (int k = 0; k < 3; ++k)
             if (k < rest) dens_one(__ldg(xs + (ent[k] & kRowIndexMask)), xi, k_, a);
     }
+    for (int e = na; e < na_all; ++e) dens_one(__ldg(xs + (tl.entry(s, e - na) & kRowIndexMask)), xi, k_, a);
     const float rho = a.rho.x + a.rho.y, sg = a.sg.x + a.sg.y;
     const float gx = a.gx.x + a.gx.y, gy = a.gy.x + a.gy.y, gz = a.gz.x + a.gz.y;
     float l = sg + (gx * gx + gy * gy + gz * gz);
@@ -285,12 +300,12 @@ __device__ __forceinline__ void disp_one(const float4& a, int v, const float4& x
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
     k_pass_disp2(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
-                 int row_cap, int n, PassK k_, float4* __restrict__ xs_out)
+                 int row_cap, int n, PassK k_, float4* __restrict__ xs_out, Tail tl)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float4 xi = xl[s];
-    const int nu = rcnt[s].y;
+    const int nu_all = rcnt[s].y, nu = min(nu_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     DispAcc a{};
     const int nfull = nu >> 2, nq = (nu + 3) >> 2;
@@ -313,6 +328,10 @@ __global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
 #pragma unroll
         for (int k = 0; k < 3; ++k)
             if (k < rest) disp_one(__ldg(xl + (ent[k] & kRowIndexMask)), ent[k], xi, k_, a);
+    }
+    for (int e = nu; e < nu_all; ++e) {
+        const int v = tl.entry(s, e - nu);
+        disp_one(__ldg(xl + (v & kRowIndexMask)), v, xi, k_, a);
     }
     // the sums hold -(displacement): d was x_j - x_i
     xs_out[s] = make_float4(xi.x - (a.ax.x + a.ax.y), xi.y - (a.ay.x + a.ay.y), xi.z - (a.az.x + a.az.y), 0.f);
@@ -366,14 +385,26 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
     k_pass_visc(const float4* __restrict__ xs, const float4* __restrict__ vin, const float4* __restrict__ vold,
                 const int* __restrict__ rows, const int2* __restrict__ rcnt, int row_cap, int n, ViscK k_,
-                float4* __restrict__ vout)
+                float4* __restrict__ vout, Tail tl)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float4 xi = xs[s];
-    const int na = rcnt[s].x;
+    const int na_all = rcnt[s].x, na = min(na_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
     float tw = 0.f, dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
+    auto pair = [&](int v) {
+        const int j = v & kRowIndexMask;
+        const float4 xj = __ldg(xs + j);
+        const float4 vj = __ldg(vin + j);
+        float d2, ir, dd;
+        pair_geom(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, k_.inv_h, d2, ir, dd);
+        const float w = d2 > kEps2 ? k_.cw * dd : 0.0f;
+        tw += w;
+        dx_ = fmaf(w, vj.x, dx_);
+        dy_ = fmaf(w, vj.y, dy_);
+        dz_ = fmaf(w, vj.z, dz_);
+    };
     const int nq = (na + 3) >> 2;
     int4 ring[kPassPrefetch];  // ring[k] = quad q + k of the row
 #pragma unroll
@@ -387,18 +418,10 @@ __global__ void __launch_bounds__(BLOCK)
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (4 * q + k >= na) break;
-            const int j = ent[k] & kRowIndexMask;
-            const float4 xj = __ldg(xs + j);
-            const float4 vj = __ldg(vin + j);
-            float d2, ir, dd;
-            pair_geom(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, k_.inv_h, d2, ir, dd);
-            const float w = d2 > kEps2 ? k_.cw * dd : 0.0f;
-            tw += w;
-            dx_ = fmaf(w, vj.x, dx_);
-            dy_ = fmaf(w, vj.y, dy_);
-            dz_ = fmaf(w, vj.z, dz_);
+            pair(ent[k]);
         }
     }
+    for (int e = na; e < na_all; ++e) pair(tl.entry(s, e - na));
     const float b = tw < kEpsilon ? 0.0f : k_.b;
     const float t = tw < kEpsilon ? 1.0f : tw;
     const float4 vo = vold[s];
@@ -458,25 +481,25 @@ static void by_block(int block, Args&&... args)
 template <int B>
 struct LaunchDensity {
     static void run(unsigned nb, cudaStream_t st, const float4* cur, const int* rows, const int2* rcnt, int row_cap,
-                    int n, PassK pk, float4* xl, float* rho)
+                    int n, PassK pk, float4* xl, float* rho, Tail tl)
     {
-        k_pass_density2<B><<<nb, B, 0, st>>>(cur, rows, rcnt, row_cap, n, pk, xl, rho);
+        k_pass_density2<B><<<nb, B, 0, st>>>(cur, rows, rcnt, row_cap, n, pk, xl, rho, tl);
     }
 };
 template <int B>
 struct LaunchDisp {
     static void run(unsigned nb, cudaStream_t st, const float4* xl, const int* rows, const int2* rcnt, int row_cap,
-                    int n, PassK pk, float4* out)
+                    int n, PassK pk, float4* out, Tail tl)
     {
-        k_pass_disp2<B><<<nb, B, 0, st>>>(xl, rows, rcnt, row_cap, n, pk, out);
+        k_pass_disp2<B><<<nb, B, 0, st>>>(xl, rows, rcnt, row_cap, n, pk, out, tl);
     }
 };
 template <int B>
 struct LaunchVisc {
     static void run(unsigned nb, cudaStream_t st, const float4* xs, const float4* vin, const float4* vold,
-                    const int* rows, const int2* rcnt, int row_cap, int n, ViscK vk, float4* vout)
+                    const int* rows, const int2* rcnt, int row_cap, int n, ViscK vk, float4* vout, Tail tl)
     {
-        k_pass_visc<B><<<nb, B, 0, st>>>(xs, vin, vold, rows, rcnt, row_cap, n, vk, vout);
+        k_pass_visc<B><<<nb, B, 0, st>>>(xs, vin, vold, rows, rcnt, row_cap, n, vk, vout, tl);
     }
 };
 
@@ -490,6 +513,7 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     int launches = 0;
     const float4* cur = c->xs0;
     const PassK pk = pass_k(k, mass);
+    const Tail tl{c->rpool, c->ovf};
     // pass B reads only xl, so it may overwrite the positions pass A read
     // (except xs0, which the velocity update needs)
     for (int it = 0; it < iterations; ++it) {
@@ -497,17 +521,17 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
         prof_begin(c, PK_PROF_DENSITY, st);
         if (PK_PASS_F32X2)
             by_block<LaunchDensity>(pb, nbp, st, cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
-                                    last ? c->rho : nullptr);
+                                    last ? c->rho : nullptr, tl);
         else
             k_pass_density<<<(n + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(
-                cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb, last ? c->rho : nullptr);
+                cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb, last ? c->rho : nullptr, tl);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
         if (PK_PASS_F32X2)
-            by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa);
+            by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa, tl);
         else
             k_pass_disp<<<(n + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt,
-                                                                                 c->row_cap, n, pk, c->xa);
+                                                                                 c->row_cap, n, pk, c->xa, tl);
         prof_end(c, PK_PROF_DISP, st);
         cur = c->xa;
         launches += 2;
@@ -522,7 +546,7 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
         float4* vin = c->vv;
         float4* vout = c->xb;
         for (int t = 0; t < vis_iterations; ++t) {
-            by_block<LaunchVisc>(pb, nbp, st, cur, vin, c->vs, c->rows, c->rcnt, c->row_cap, n, vk, vout);
+            by_block<LaunchVisc>(pb, nbp, st, cur, vin, c->vs, c->rows, c->rcnt, c->row_cap, n, vk, vout, tl);
             float4* tmp = vin;
             vin = vout;
             vout = tmp;
@@ -550,10 +574,12 @@ int pbd_replay_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iteration
     const int pb = c->tune.pass_block;
     const unsigned nb1 = (unsigned)((n + 255) / 256), nbp = (unsigned)((n + pb - 1) / pb);
     const PassK pk = pass_k(k, mass);
+    const Tail tl{c->rpool, c->ovf};  // unused: the rollout's rows fit their capacity
     for (int it = 0; it < iterations; ++it) {
         by_block<LaunchDensity>(pb, nbp, st, ys + (size_t)it * n, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
-                                nullptr);
-        by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, ys + (size_t)(it + 1) * n);
+                                nullptr, tl);
+        by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, ys + (size_t)(it + 1) * n,
+                             tl);
     }
     k_finish<<<nb1, 256, 0, st>>>(ys + (size_t)iterations * n, ys, c->vs, c->rho, c->perm, n, dt, x, v, nullptr);
     return 2 * iterations + 1;

@@ -388,7 +388,7 @@ int frame32(pk_ctx* c, const PbdRoll& R, float* x, float* v, float4* ys, cudaStr
 {
     const int n = R.n;
     int l = sort_particles(c, x, v, nullptr, n, R.g, false, nullptr, 0.f, 0.f, R.dt, true, R.p.gravity, st);
-    l += build_rows(c, n, R.g, R.p.nq.radius, R.p.nq.cap, R.row_cap, nullptr, nullptr, 0, st);
+    l += build_rows(c, n, R.g, R.p.nq.radius, R.p.nq.cap, R.row_cap, nullptr, nullptr, 0, st, false);
     if (ys)
         l += pbd_replay_solve(c, n, R.k, R.mass, R.iterations, R.dt, ys, x, v, st);
     else
@@ -407,7 +407,7 @@ int frame64(pk_ctx* c, PbdRoll& R, double* x, double* v, double4* ys, cudaStream
     k64_round<<<blocks_of(m3, 256), 256, 0, st>>>(x, m3, R.xf);
     int l = 1 + sort_particles(c, R.xf, R.xf, nullptr, n, R.g, false, nullptr, 0.f, 0.f, R.dt, false,
                                R.p.gravity, st);
-    l += build_rows(c, n, R.g, R.p.nq.radius, R.p.nq.cap, R.row_cap, nullptr, nullptr, 0, st);
+    l += build_rows(c, n, R.g, R.p.nq.radius, R.p.nq.cap, R.row_cap, nullptr, nullptr, 0, st, false);
     const double dt = (double)R.dt;
     double4* y0 = ys ? ys : R.y64a;
     k64_begin<<<blocks_of(n, 256), 256, 0, st>>>(x, v, c->perm, n, (double)R.p.gravity[0], (double)R.p.gravity[1],

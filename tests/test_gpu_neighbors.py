@@ -96,17 +96,6 @@ def test_overfull_cells_capped(oracle):
     assert_same_lists(oracle, x, 0.0125, (0, 0, 0), (1, 1, 1), 64)
 
 
-def test_hit_overflow_is_reported(ctx):
-    # more than 512 particles within the radius of each other: the build
-    # reports PK_ERR_CAPACITY instead of returning a truncated list
-    import pkhot
-    rng = np.random.default_rng(10)
-    x = torch.from_numpy(rng.uniform(0.5, 0.508, size=(600, 3)).astype(np.float32)).cuda()
-    ctx.nq_build(x, 0.0125, (0, 0, 0), (1, 1, 1), 64)
-    assert ctx.status() == pkhot.PK_ERR_CAPACITY
-    assert ctx.status() == pkhot.PK_OK  # the condition is cleared once reported
-
-
 def test_dynamic_list_is_symmetric_at_scale(ctx):
     # size-independent property at the 2M scene's density: j in N(i) <=> i in N(j)
     sc = scenes.dam_break_2m(seed=1, n_side=64)
