@@ -13,8 +13,9 @@
  *
  * All work is enqueued on `stream` (NULL = legacy default stream) without a
  * host synchronisation, except where a function says it synchronises.
- * Conditions found on the device (a row over capacity) are latched in the
- * context and reported by pk_ctx_status().
+ * Conditions found on the device (a spill pool too small for the frame's
+ * long rows, a list over its capacity) are latched in the context and
+ * reported by pk_ctx_status().
  *
  * Reference paths below are relative to PhysIKA's source tree (Source/).
  */
@@ -61,8 +62,9 @@ typedef struct {
     float lo[3];       /* scene bounds (NeighborQuery::setBoundingBox, NeighborQuery.h:30) */
     float hi[3];
     int cap;           /* setNeighborSizeLimit (NeighborQuery.h:34); 0 = dynamic list */
-    int max_neighbors; /* dynamic mode: per-particle bound (0 = 512, the maximum); any mode
-                          reports PK_ERR_CAPACITY through pk_ctx_status above 512 hits */
+    int max_neighbors; /* dynamic mode: entries per particle kept in the context's main rows
+                          (0 = 192, at most 4096; fixed mode keeps max(128, 2 cap)).  Not a
+                          limit: longer rows continue in the context's spill pool */
 } pk_nq_params;
 
 /* NeighborQuery::compute (Framework/Topology/NeighborQuery.cu:152-199):
@@ -78,7 +80,11 @@ typedef struct {
  * Dynamic mode writes CSR offsets to index[n] and, if the total fits,
  * elements; when `total` is non-NULL this call synchronises `stream` and
  * stores the number of entries (and returns PK_ERR_CAPACITY if it exceeded
- * elements_capacity, as the reference re-sizes its list, NeighborQuery.cu:463-472). */
+ * elements_capacity, as the reference re-sizes its list, NeighborQuery.cu:463-472).
+ * Any number of particles may lie inside one radius (as for the reference):
+ * rows longer than the context's row capacity continue in its spill pool, and
+ * this call synchronises `stream` once to check that the pool held them,
+ * growing it and repeating the build when it did not. */
 int pk_nq_build(pk_ctx* ctx, const float* x, int n, const pk_nq_params* p,
                 int* index, int* elements, long long elements_capacity,
                 long long* total, pk_stream stream);
@@ -204,7 +210,11 @@ typedef struct {
  * integrator begin, NeighborQuery on the current positions, integrate,
  * DensityPBD, and ImplicitViscosity when p->viscosity > 0.
  * x, v (n AoS) are updated in place; rho_out may be NULL.  Asynchronous and
- * allocation-free once the context has seen `n` (capturable in a CUDA graph). */
+ * allocation-free once the context has seen `n` (capturable in a CUDA graph).
+ * Rows longer than the row capacity continue in the context's spill pool
+ * (8 entries per particle at first); a frame that needs more reports
+ * PK_ERR_CAPACITY through pk_ctx_status, which records the size, and the
+ * next frame runs with the pool grown to it. */
 int pk_pbf_step(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p,
                 float* rho_out, pk_stream stream);
 
@@ -414,7 +424,8 @@ int pk_pd_rollout_backward_f64(pk_ctx* ctx, const double* xbar, const double* vb
  * at the start of every checkpoint_every-th step (0: only the first) is kept
  * on the context for pk_pbd_rollout_backward.  A frame's list is a step
  * constant: the derivative is that of the frame map with the list frozen.
- * Rows hold at most 128 hits per particle (beyond, pk_ctx_status reports
+ * Rows hold at most 128 hits per particle (the frames' rows are kept for the
+ * reverse pass, so a longer row is not spilled: pk_ctx_status reports
  * PK_ERR_CAPACITY). */
 int pk_pbd_rollout(pk_ctx* ctx, float* x, float* v, int n, const pk_pbf_params* p, int steps,
                    int checkpoint_every, pk_stream stream);

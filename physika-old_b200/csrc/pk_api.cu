@@ -98,13 +98,15 @@ int ensure_pool(pk_ctx* c, int n)
 }
 
 // Entries the last build handed out of the spill pool (also past its
-// capacity); stream-ordered read, so the caller has synchronised.
-long long spill_used(pk_ctx* c, cudaStream_t st)
+// capacity), read after the stream's work; with offs_n, the dynamic list's
+// total too, in the same synchronisation.  -1 on a CUDA error.
+long long spill_used(pk_ctx* c, cudaStream_t st, int n = 0, int* offs_n = nullptr)
 {
     unsigned long long used = 0;
-    if (cudaMemcpyAsync(&used, c->spill, sizeof(used), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return -1;
+    cudaError_t e = cudaMemcpyAsync(&used, c->spill, sizeof(used), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && offs_n) e = cudaMemcpyAsync(offs_n, c->offs + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return -1;
     if ((long long)used > c->pool_cap) c->pool_need = std::max(c->pool_need, (long long)used);
     return (long long)used;
 }
@@ -143,13 +145,14 @@ int ensure_generic(pk_ctx* c, int n)
 }
 
 // Entries per particle kept in the main hit and solver rows: 128, or 2 cap
-// for a larger cap, or a dynamic list's max_neighbors (a multiple of 4).
-// Longer rows continue in the spill pool.
+// for a larger cap; a dynamic list, whose solver rows hold every hit, 192 or
+// its max_neighbors (a multiple of 4).  Longer rows continue in the spill
+// pool.
 int row_capacity(const pk_nq_params* p)
 {
     int m = pk::kRowCapMin;
     if (p->cap > 0) m = std::max(m, 2 * p->cap);
-    if (p->cap <= 0 && p->max_neighbors > 0) m = std::max(m, p->max_neighbors);
+    if (p->cap <= 0) m = p->max_neighbors > 0 ? std::max(m, p->max_neighbors) : pk::kRowCapDynamic;
     return std::min((m + 3) & ~3, pk::kRowCapMax);
 }
 
@@ -423,6 +426,8 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
     // rows longer than the capacity go to the spill pool; a pool too small for
     // this build is grown to what the build asked for and the build repeated
     int launches = 0;
+    const bool dyn_total = total && p->cap <= 0 && index;
+    int t = 0;  // the dynamic list's total, read in the same synchronisation
     for (int attempt = 0; attempt < 2; ++attempt) {
         if ((rc = ensure_pool(c, n))) return rc;
         launches = pk::sort_particles(c, const_cast<float*>(x), nullptr, nullptr, n, g, false, nullptr, 0.f, 0.f,
@@ -430,7 +435,7 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
         launches += pk::build_rows(c, n, g, p->radius, p->cap, row_cap, index, elements,
                                    elements ? elements_capacity : 0, st);
         if ((rc = check_launch(c, "pk_nq_build"))) return rc;
-        const long long used = spill_used(c, st);
+        const long long used = spill_used(c, st, n, dyn_total && n > 0 ? &t : nullptr);
         if (used < 0) return cuda_fail(c, cudaGetLastError(), "pk_nq_build");
         if (used <= c->pool_cap) break;
         cudaMemset(c->d_err, 0, sizeof(int));  // the repeated build replaces this one
@@ -441,10 +446,6 @@ PK_API int pk_nq_build(pk_ctx* c, const float* x, int n, const pk_nq_params* p, 
         if (p->cap > 0) {
             *total = (long long)n * p->cap;
         } else if (index) {
-            int t = 0;
-            cudaError_t e = cudaMemcpyAsync(&t, c->offs + n, sizeof(int), cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) return cuda_fail(c, e, "pk_nq_build");
             *total = n > 0 ? t : 0;
             if (elements && *total > elements_capacity) {
                 cudaMemset(c->d_err, 0, sizeof(int));

@@ -25,11 +25,15 @@ constexpr int kRowFlagA = 1 << 31;
 constexpr int kRowFlagB = 1 << 30;
 constexpr int kRowIndexMask = (1 << 30) - 1;
 // Per-particle row capacity of the hit rows and solver rows held in the main
-// arrays (kRowCapMin, or 2 cap for a larger cap, or a dynamic list's
-// max_neighbors).  A particle with more hits keeps the rest of its hit row and
+// arrays (kRowCapMin, or 2 cap for a larger cap; kRowCapDynamic or
+// max_neighbors for a dynamic list).  A particle with more hits keeps the rest of its hit row and
 // of its solver row in the spill pool, so no count of particles inside one
 // radius is too large for a list.
-constexpr int kRowCapMin = 128;
+#ifndef PK_ROWCAP_MIN
+#define PK_ROWCAP_MIN 128
+#endif
+constexpr int kRowCapMin = PK_ROWCAP_MIN;
+constexpr int kRowCapDynamic = 192;  // dynamic lists by default (every hit is a row entry)
 constexpr int kRowCapMax = 4096;
 
 // Solver rows are interleaved by blocks of 32 sorted particles and quads of

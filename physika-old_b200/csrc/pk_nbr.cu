@@ -30,10 +30,10 @@
 //   k_spill (particles with more hits than the row capacity): the same sweep
 //     for one particle, keeping the hits past the capacity in the particle's
 //     segment of the spill pool, so a row of any length is in candidate order.
-//   k_emit (one thread per particle): re-reads the hit row a quad at a time,
-//     marks a = key <= tau_i (j in N(i)) and b = key' <= tau_j (i in N(j)),
-//     writes the solver row with a-entries first, then b-only entries, and the
-//     public NeighborList in caller ids (fixed: index = count; dynamic: CSR).
+//   k_emit (8 lanes per particle): re-reads the hit row, marks a = key <= tau_i
+//     (j in N(i)) and b = key' <= tau_j (i in N(j)), compacts in place with
+//     a-entries first, then b-only entries, and writes the public NeighborList
+//     in caller ids (fixed: index = count; dynamic: CSR).
 // Distances use the explicit roundings of exact_norm3's squared sum, so every
 // d < h decision and every ordering is bit-identical for (i, j) and (j, i)
 // and matches the CPU restatement.
@@ -172,31 +172,56 @@ __device__ __forceinline__ int sweep_ranges(const BuildArgs& A, SweepSmem& S, in
     return total;
 }
 
-// One pass of the sweep: kPB particles in registers against every candidate
-// chunk.  kChecked guards the row bound; a cell whose 27 ranges hold at most
-// row_cap candidates cannot overflow a row and runs unchecked.
+// One chunk of 32 candidates against the pass's particles.  kChecked guards
+// the row bound (hits past it are counted, and written by k_spill).
 template <bool kChecked, int KPB>
+__device__ __forceinline__ void sweep_chunk(const BuildArgs& A, uint2* row0, const float4& cx, int t, int m,
+                                            const float (&px)[KPB], const float (&py)[KPB],
+                                            const float (&pz)[KPB], int (&cnt)[KPB], unsigned lt)
+{
+#pragma unroll
+    for (int p = 0; p < KPB; ++p) {
+        if (p >= m) break;  // warp-uniform
+        const float d2 = exact_d2(make_float4(px[p], py[p], pz[p], 0.f), cx);
+        const bool hit = d2 < A.T;
+        const unsigned b = __ballot_sync(kFull, hit);
+        const int pos = cnt[p] + __popc(b & lt);
+        if (hit && (!kChecked || pos < A.row_cap))
+            row0[p * A.row_cap + pos] = make_uint2((unsigned)t, __float_as_uint(d2));
+        cnt[p] += __popc(b);
+    }
+}
+
+// One pass of the sweep: kPB particles in registers against every candidate
+// chunk.  A chunk adds at most 32 hits to a row, so with the pass's largest
+// count at c the next (row_cap - c) / 32 chunks cannot overflow a row: they
+// run as an unchecked loop, after which the bound is refreshed; chunks left
+// when no row has 32 entries to spare run checked.  (Counts are
+// warp-uniform.  Deciding checked or not inside one loop, per chunk, cost
+// 14% more instructions.)
+template <int KPB>
 __device__ __forceinline__ void sweep(const BuildArgs& A, const SweepSmem& S, int total, int p0, int m,
                                       const float (&px)[KPB], const float (&py)[KPB], const float (&pz)[KPB],
                                       int (&cnt)[KPB], int lane, unsigned lt)
 {
     uint2* const row0 = A.hits + (long long)p0 * A.row_cap;
-    for (int c0 = 0; c0 < total; c0 += 32) {
+    int c0 = 0;
+    while (c0 < total) {
+        int mx = 0;
+#pragma unroll
+        for (int p = 0; p < KPB; ++p) mx = max(mx, cnt[p]);
+        const int run_end = min(total, c0 + ((A.row_cap - mx) >> 5) * 32);
+        if (run_end <= c0) break;
+        for (; c0 < run_end; c0 += 32) {
+            int t;
+            const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
+            sweep_chunk<false, KPB>(A, row0, cx, t, m, px, py, pz, cnt, lt);
+        }
+    }
+    for (; c0 < total; c0 += 32) {
         int t;
         const float4 cx = fetch_cand(A.xs, S, c0 + lane, total, t);
-        auto append = [&](int p, float d2) {
-            const bool hit = d2 < A.T;
-            const unsigned b = __ballot_sync(kFull, hit);
-            const int pos = cnt[p] + __popc(b & lt);
-            if (hit && (!kChecked || pos < A.row_cap))
-                row0[p * A.row_cap + pos] = make_uint2((unsigned)t, __float_as_uint(d2));
-            cnt[p] += __popc(b);
-        };
-#pragma unroll
-        for (int p = 0; p < KPB; ++p) {
-            if (p >= m) break;  // warp-uniform
-            append(p, exact_d2(make_float4(px[p], py[p], pz[p], 0.f), cx));
-        }
+        sweep_chunk<true, KPB>(A, row0, cx, t, m, px, py, pz, cnt, lt);
     }
 }
 
@@ -244,10 +269,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32, build_min_blocks<KPB>()) k_b
                 }
                 cnt[p] = 0;
             }
-            if (total <= A.row_cap)
-                sweep<false, KPB>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
-            else
-                sweep<true, KPB>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
+            sweep<KPB>(A, S, total, p0, m, px, py, pz, cnt, lane, lt);
 #pragma unroll
             for (int p = 0; p < KPB; ++p) {
                 if (lane == p && p < m) {
@@ -295,6 +317,11 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_spill(BuildArgs A)
 constexpr int kSelWarps = 8;
 constexpr int kSelRegChunks = 4;  // rows of up to 128 hits are held in registers
 
+// Hit e of a row held wholly in the main array.
+struct PtrRow {
+    const uint2* row;
+    __device__ __forceinline__ uint2 at(int e) const { return __ldg(row + e); }
+};
 // Hit e of one particle's row: the main array up to the row capacity, then
 // the particle's spill segment.
 struct HitRow {
@@ -328,8 +355,8 @@ __device__ __forceinline__ int sel_bin(unsigned db, float lo, float scale)
 // exactly by (d2, index); more than 32 hits at one d2 value are ranked by
 // index.  Src supplies the row: chunk k of 32 entries (lanes past c hold
 // d2 bits 0xffffffff, outside every interval).
-template <class Src>
-__device__ __forceinline__ uint2 select_rank(const Src& src, int nch, const HitRow& row, int c, int rr, float T,
+template <class Src, class Row>
+__device__ __forceinline__ uint2 select_rank(const Src& src, int nch, const Row& row, int c, int rr, float T,
                                              SelSmem& S, int lane, unsigned lt)
 {
     unsigned plo = 0u, phi = __float_as_uint(T);  // [0, T]: every hit
@@ -549,12 +576,7 @@ __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
             const int q = __ffs(need) - 1;
             need &= need - 1;
             const int c = __shfl_sync(kFull, c_l, q);
-            const long long sq = base + q;
-            HitRow row{hits + sq * row_cap, nullptr, row_cap};
-            if (c > row_cap) {
-                const int o = __ldg(ovf + sq);
-                row.pool = o >= 0 ? hpool + o : nullptr;
-            }
+            const uint2* row = hits + (base + q) * row_cap;
             uint2 h[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) h[k] = hn[k];
@@ -569,9 +591,15 @@ __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
                     const int e = k * 32 + lane;
                     src.h[k] = e < c ? h[k] : make_uint2(0u, 0xffffffffu);
                 }
-                r = select_rank(src, (c + 31) / 32, row, c, cap - 1, T, S, lane, lt);
+                r = select_rank(src, (c + 31) / 32, PtrRow{row}, c, cap - 1, T, S, lane, lt);
             } else {
-                r = select_rank(MemSrc{row, c, lane}, (c + 31) / 32, row, c, cap - 1, T, S, lane, lt);
+                // rows past the row capacity continue in their spill segment
+                HitRow hr{row, nullptr, row_cap};
+                if (c > row_cap && hpool) {
+                    const int o = __ldg(ovf + base + q);
+                    if (o >= 0) hr.pool = hpool + o;
+                }
+                r = select_rank(MemSrc{hr, c, lane}, (c + 31) / 32, hr, c, cap - 1, T, S, lane, lt);
             }
             if (lane == q) tau_l = r;
         }
@@ -580,21 +608,32 @@ __global__ void __launch_bounds__(kSelWarps * 32, PK_SEL_MIN_BLOCKS)
     }
 }
 
-// Solver rows from the hit rows, one thread per particle.  The thread reads
-// its hit row two quads (8 hits, 64 contiguous bytes) at a time, gathers
-// tau_j of those hits (L2-resident), marks a and b, and writes its solver
-// row a quad (16 bytes) at a time into the interleaved layout: a-entries in
-// hit order, then the b-only entries, which wait in shared memory (kEmitStash
-// per thread; a second walk over the row picks up any beyond).  Rows longer
-// than the capacity continue in the particle's spill segment.
-constexpr int kEmitBlock = 256;
-constexpr int kEmitStash = 16;
+// Solver rows from the hit rows: G lanes per particle.  k_emit takes the
+// rows that fit the row capacity (all but the longest); k_emit_spill the
+// particles listed with a spill segment, whose hits and solver entries past
+// the capacity live there.
+constexpr int kEmitG = 8;
+constexpr int kStash = 128;  // b-only entries kept per group before appending (>= kRowCapMin)
+// Chunks of kEmitG entries whose loads are issued together, and resident
+// blocks per SM asked of the register allocator: 2 chunks at 8 blocks (32
+// registers) measured fastest at 2M, ahead of 1, 3 or 4 chunks at 4-6 blocks,
+// and ahead of one thread per particle reading a quad of hits per load
+// (0.72-0.81 against 0.66 ms at 2M).
+#ifndef PK_EMIT_U
+#define PK_EMIT_U 2
+#endif
+#ifndef PK_EMIT_MINB
+#define PK_EMIT_MINB 8
+#endif
+constexpr int kEmitU = PK_EMIT_U;
 
 struct EmitArgs {
     const int* hcnt;
     const uint2* hits;
     const uint2* hpool;  // null: no spill pool
     const int* ovf;
+    const unsigned long long* spill;
+    const int* ovf_list;
     const uint2* tau;
     const int* perm;
     int n, cap, rc;
@@ -608,126 +647,206 @@ struct EmitArgs {
     int* err;
 };
 
-// One particle's solver row, written in order a quad at a time.
-struct RowOut {
-    int4* q0;   // quad 0 of the particle's interleaved row (its quads are 32 apart)
-    int* pool;  // the particle's spill segment, or null
-    int rc, len;
-    int4 pend;
-    bool over;
-    __device__ __forceinline__ void flush(int q)
-    {
-        if (4 * q < rc)
-            q0[32LL * q] = pend;
-        else if (pool)
-            *reinterpret_cast<int4*>(pool + (4 * q - rc)) = pend;
-        else
-            over = true;
-    }
-    __device__ __forceinline__ void put(int v)
-    {
-        const int k = len & 3;
-        if (k == 0) pend.x = v;
-        if (k == 1) pend.y = v;
-        if (k == 2) pend.z = v;
-        if (k == 3) pend.w = v;
-        ++len;
-        if ((len & 3) == 0) flush((len >> 2) - 1);
-    }
-    __device__ __forceinline__ void finish()
-    {
-        if (len & 3) flush(len >> 2);
-    }
-};
-
-__global__ void __launch_bounds__(kEmitBlock) k_emit(EmitArgs A)
+__global__ void __launch_bounds__(256, PK_EMIT_MINB) k_emit(EmitArgs A)
 {
-    __shared__ int stash[kEmitStash][kEmitBlock];
-    const int s = blockIdx.x * kEmitBlock + threadIdx.x;
-    if (s >= A.n) return;  // no warp-wide operation follows
+    __shared__ int s_b[256 / kEmitG][kStash];  // b-only entries of each group
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = gid / kEmitG, sub = gid % kEmitG, grp = threadIdx.x / kEmitG;
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = ((1u << kEmitG) - 1u) << (lane & ~(kEmitG - 1));
+    const unsigned lt_g = ((1u << lane) - 1u) & gmask;
+    int cnt = s < A.n ? A.hcnt[s] : 0;
+    bool valid = s < A.n;
+    if (valid && cnt > A.rc) {
+        if (A.hpool && __ldg(A.ovf + s) >= 0)
+            valid = false;  // k_emit_spill's
+        else
+            cnt = A.rc;     // no segment could be had: cut short, the error is latched
+    }
+    if (!valid) cnt = 0;
     const bool capped = A.cap > 0;
-    const int c = A.hcnt[s];
-    const uint2 ti = capped ? A.tau[s] : make_uint2(0x7f800000u, 0x7fffffffu);
-    const int ps = A.perm[s];
+    int ps = 0;
+    uint2 ti = make_uint2(0x7f800000u, 0x7fffffffu);
+    long long pbase = 0;
     const bool pub = A.pub_elements != nullptr;
-    const long long pbase = pub ? (capped ? (long long)ps * A.cap : (long long)A.offs[ps]) : 0;
-    const uint2* hrow = A.hits + (long long)s * A.rc;
-    const int o = (c > A.rc && A.hpool) ? A.ovf[s] : -1;
-    const uint2* hseg = o >= 0 ? A.hpool + o : nullptr;
-    // hits past the capacity are lost only when the pool ran out (latched by the build)
-    const int cm = (c > A.rc && !hseg) ? A.rc : c;
-    RowOut out;
-    out.q0 = reinterpret_cast<int4*>(A.rows) + (long long)(s >> 5) * row_quads(A.rc) * 32 + (s & 31);
-    out.pool = o >= 0 ? A.rpool + o : nullptr;
-    out.rc = A.rc;
-    out.len = 0;
-    out.pend = make_int4(0, 0, 0, 0);
-    out.over = false;
-    bool pub_over = false;
-    int nB = 0;
-    for (int e0 = 0; e0 < cm; e0 += 8) {
-        uint2 h[8], tj[8];
+    if (valid) {
+        if (capped) ti = A.tau[s];
+        ps = A.perm[s];
+        if (pub) pbase = capped ? (long long)ps * A.cap : (long long)A.offs[ps];
+    }
+    const int so = valid ? s : 0;
+    const uint2* hrow = A.hits + (long long)so * A.rc;
+    // every lane of the warp iterates to the longest row of the warp's groups
+    int cmax = cnt;
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const int e = e0 + 4 * u;  // a quad lies wholly in the main row or in the segment
-            uint4 a = make_uint4(0u, 0u, 0u, 0u), b = a;
-            if (e < cm) {
-                const uint2* src = e < A.rc ? hrow + e : hseg + (e - A.rc);
-                a = __ldg(reinterpret_cast<const uint4*>(src));
-                b = __ldg(reinterpret_cast<const uint4*>(src + 2));
-            }
-            h[4 * u] = make_uint2(a.x, a.y);
-            h[4 * u + 1] = make_uint2(a.z, a.w);
-            h[4 * u + 2] = make_uint2(b.x, b.y);
-            h[4 * u + 3] = make_uint2(b.z, b.w);
+    for (int o = 16; o >= 1; o >>= 1) cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
+    int nA = 0, nB = 0;
+    bool over = false;
+    // kEmitU chunks per round: their hit loads, then their tau_j gathers, are
+    // all in flight before the first ballot (the chunks are then decided and
+    // written in order, as one chunk at a time would)
+    for (int e0 = 0; e0 < cmax; e0 += kEmitG * kEmitU) {
+        uint2 h[kEmitU], tj[kEmitU];
+#pragma unroll
+        for (int u = 0; u < kEmitU; ++u) {
+            const int e = e0 + u * kEmitG + sub;
+            h[u] = (valid && e < cnt) ? __ldg(hrow + e) : make_uint2(0u, 0u);
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) tj[k] = (capped && e0 + k < cm) ? __ldg(A.tau + h[k].x) : make_uint2(0u, 0u);
+        for (int u = 0; u < kEmitU; ++u) {
+            const int e = e0 + u * kEmitG + sub;
+            tj[u] = (capped && valid && e < cnt) ? __ldg(A.tau + h[u].x) : make_uint2(0u, 0u);
+        }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (e0 + k >= cm) break;
-            const int t = (int)h[k].x;
-            bool fa = true, fb = true;
-            if (capped) {
-                const float d2 = __uint_as_float(h[k].y);
-                fa = key_le(d2, t, ti);
-                fb = key_le(d2, s, tj[k]);
+        for (int u = 0; u < kEmitU; ++u) {
+            if (e0 + u * kEmitG >= cmax) break;  // warp-uniform: cmax is the warp's maximum
+            const int e = e0 + u * kEmitG + sub;
+            bool fa = false, fb = false;
+            const int t = (int)h[u].x;
+            if (valid && e < cnt) {
+                if (capped) {
+                    const float d2 = __uint_as_float(h[u].y);
+                    fa = key_le(d2, t, ti);
+                    fb = key_le(d2, s, tj[u]);
+                } else {
+                    fa = fb = true;
+                }
             }
+            const unsigned ba = __ballot_sync(kFull, fa) & gmask;
+            const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
             if (fa) {
+                const int q = nA + __popc(ba & lt_g);
+                A.rows[row_slot(so, q, A.rc)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
                 if (pub) {
-                    const long long po = pbase + out.len;
-                    if (capped ? (out.len < A.cap) : (po < A.pub_capacity))
+                    const long long o = pbase + q;
+                    if (capped ? (q < A.cap) : (o < A.pub_capacity))
+                        A.pub_elements[o] = __ldg(A.perm + t);
+                    else
+                        over = true;
+                }
+            }
+            if (fb && !fa) {
+                // a row of at most rc <= kStash hits has at most kStash b-only entries
+                const int q = nB + __popc(bb & lt_g);
+                s_b[grp][q] = t | kRowFlagB;
+            }
+            nA += __popc(ba);
+            nB += __popc(bb);
+        }
+    }
+    __syncwarp();
+    if (valid) {
+        for (int e = sub; e < nB; e += kEmitG) A.rows[row_slot(so, nA + e, A.rc)] = s_b[grp][e];
+        if (sub == 0) {
+            A.rcnt[s] = make_int2(nA, nA + nB);
+            if (A.pub_index != nullptr) A.pub_index[ps] = capped ? min(nA, A.cap) : A.offs[ps];
+        }
+    }
+    if (__any_sync(kFull, over) && lane == 0) atomicOr(A.err, kErrPublicOverflow);
+}
+
+// The same for the particles listed with a spill segment (rows longer than
+// the capacity: dense clusters only), a warp per four of them: hits and
+// solver entries numbered rc and up are in the segment, and b-only entries
+// past the stash are taken by a second walk over the row.
+__global__ void __launch_bounds__(256) k_emit_spill(EmitArgs A)
+{
+    __shared__ int s_b[256 / kEmitG][kStash];
+    const int lane = threadIdx.x & 31, sub = lane % kEmitG, grp = threadIdx.x / kEmitG;
+    const unsigned gmask = ((1u << kEmitG) - 1u) << (lane & ~(kEmitG - 1));
+    const unsigned lt_g = ((1u << lane) - 1u) & gmask;
+    const long long listed = (long long)*A.spill;
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const bool capped = A.cap > 0;
+    const bool pub = A.pub_elements != nullptr;
+    for (long long r0 = w * 4; r0 < listed; r0 += nwarp * 4) {
+        const long long item = r0 + lane / kEmitG;
+        const bool valid = item < listed;
+        const int s = valid ? A.ovf_list[item] : 0;
+        const int cnt = valid ? A.hcnt[s] : 0;
+        const int o = valid ? A.ovf[s] : 0;
+        const uint2 ti = (valid && capped) ? A.tau[s] : make_uint2(0x7f800000u, 0x7fffffffu);
+        const int ps = valid ? A.perm[s] : 0;
+        const long long pbase = (valid && pub) ? (capped ? (long long)ps * A.cap : (long long)A.offs[ps]) : 0;
+        const uint2* hrow = A.hits + (long long)s * A.rc;
+        auto hit = [&](int e) { return e < A.rc ? __ldg(hrow + e) : __ldg(A.hpool + o + (e - A.rc)); };
+        auto put = [&](int q, int v) {
+            if (q < A.rc)
+                A.rows[row_slot(s, q, A.rc)] = v;
+            else
+                A.rpool[o + (q - A.rc)] = v;
+        };
+        int cmax = cnt;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) cmax = max(cmax, __shfl_xor_sync(kFull, cmax, off));
+        int nA = 0, nB = 0;
+        bool over = false;
+        for (int e0 = 0; e0 < cmax; e0 += kEmitG) {
+            const int e = e0 + sub;
+            bool fa = false, fb = false;
+            int t = 0;
+            if (valid && e < cnt) {
+                const uint2 h = hit(e);
+                t = (int)h.x;
+                if (capped) {
+                    const float d2 = __uint_as_float(h.y);
+                    fa = key_le(d2, t, ti);
+                    fb = key_le(d2, s, __ldg(A.tau + t));
+                } else {
+                    fa = fb = true;
+                }
+            }
+            const unsigned ba = __ballot_sync(kFull, fa) & gmask;
+            const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
+            if (fa) {
+                const int q = nA + __popc(ba & lt_g);
+                put(q, t | kRowFlagA | (fb ? kRowFlagB : 0));
+                if (pub) {
+                    const long long po = pbase + q;
+                    if (capped ? (q < A.cap) : (po < A.pub_capacity))
                         A.pub_elements[po] = __ldg(A.perm + t);
                     else
-                        pub_over = true;
+                        over = true;
                 }
-                out.put(t | kRowFlagA | (fb ? kRowFlagB : 0));
-            } else if (fb) {
-                if (nB < kEmitStash) stash[nB][threadIdx.x] = t | kRowFlagB;
-                ++nB;
+            }
+            if (fb && !fa) {
+                const int q = nB + __popc(bb & lt_g);
+                if (q < kStash) s_b[grp][q] = t | kRowFlagB;
+            }
+            nA += __popc(ba);
+            nB += __popc(bb);
+        }
+        __syncwarp();
+        if (valid)
+            for (int e = sub; e < min(nB, kStash); e += kEmitG) put(nA + e, s_b[grp][e]);
+        __syncwarp();
+        if (__any_sync(kFull, nB > kStash)) {
+            int kb = 0;
+            for (int e0 = 0; e0 < cmax; e0 += kEmitG) {
+                const int e = e0 + sub;
+                bool fbo = false;
+                int t = 0;
+                if (valid && nB > kStash && e < cnt) {
+                    const uint2 h = hit(e);
+                    t = (int)h.x;
+                    const float d2 = __uint_as_float(h.y);
+                    fbo = !key_le(d2, t, ti) && key_le(d2, s, __ldg(A.tau + t));
+                }
+                const unsigned bb = __ballot_sync(kFull, fbo) & gmask;
+                if (fbo) {
+                    const int q = kb + __popc(bb & lt_g);
+                    if (q >= kStash) put(nA + q, t | kRowFlagB);
+                }
+                kb += __popc(bb);
             }
         }
-    }
-    const int nA = out.len;
-    const int nS = min(nB, kEmitStash);
-    for (int k = 0; k < nS; ++k) out.put(stash[k][threadIdx.x]);
-    if (nB > kEmitStash) {
-        // the b-only entries past the stash, in hit order (capped lists only)
-        int seen = 0;
-        for (int e = 0; e < cm; ++e) {
-            const uint2 hh = e < A.rc ? __ldg(hrow + e) : __ldg(hseg + (e - A.rc));
-            const float d2 = __uint_as_float(hh.y);
-            const int t = (int)hh.x;
-            if (key_le(d2, t, ti) || !key_le(d2, s, __ldg(A.tau + t))) continue;
-            if (seen++ >= kEmitStash) out.put(t | kRowFlagB);
+        if (valid && sub == 0) {
+            A.rcnt[s] = make_int2(nA, nA + nB);
+            if (A.pub_index != nullptr) A.pub_index[ps] = capped ? min(nA, A.cap) : A.offs[ps];
         }
+        if (__any_sync(kFull, over) && lane == 0) atomicOr(A.err, kErrPublicOverflow);
     }
-    out.finish();
-    // a row cut short (no spill segment) reports what it holds; the error is latched
-    A.rcnt[s] = out.over ? make_int2(min(nA, A.rc), min(out.len, A.rc)) : make_int2(nA, out.len);
-    if (A.pub_index != nullptr) A.pub_index[ps] = capped ? min(nA, A.cap) : A.offs[ps];
-    if (out.over) atomicOr(A.err, kErrRowOverflow);
-    if (pub_over) atomicOr(A.err, kErrPublicOverflow);
 }
 
 // Smallest float T with sqrt_rn(T) >= h: for every float d2, sqrt_rn(d2) < h
@@ -814,6 +933,8 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     E.hits = c->hits;
     E.hpool = hpool;
     E.ovf = c->ovf;
+    E.spill = c->spill + 1;
+    E.ovf_list = c->ovf_list;
     E.tau = c->tau;
     E.perm = c->perm;
     E.n = n;
@@ -827,7 +948,11 @@ int build_rows(pk_ctx* c, int n, const Grid& g, float h, int cap, int row_cap, i
     E.pub_capacity = pub_capacity;
     E.offs = c->offs;
     E.err = c->d_err;
-    k_emit<<<(unsigned)((n + kEmitBlock - 1) / kEmitBlock), kEmitBlock, 0, st>>>(E);
+    k_emit<<<(unsigned)(((long long)n * kEmitG + 255) / 256), 256, 0, st>>>(E);
+    if (hpool) {
+        k_emit_spill<<<sms, 256, 0, st>>>(E);  // an empty launch when no row is that long
+        ++launches;
+    }
     prof_end(c, PK_PROF_EMIT, st);
     return launches + 1;
 }
