@@ -263,13 +263,17 @@ int pk_last_launch_count(const pk_ctx* ctx);
 
 /* Autotuning of the frame kernels (no reference counterpart).  With enable,
  * the next four pk_pbf_step / pk_pbf_step_batched calls are trial frames: they
- * run the Jacobi passes at 128, 256 and 512 threads per block and the
- * neighbour sweep with 4, 8 and 16 particles per pass, time them (each trial
- * frame synchronises its stream, so do not capture them in a graph), and keep
- * the fastest shapes for the context.  The shapes change no result.
- * pk_ctx_tuning reports the shapes in use and whether trials remain. */
+ * run the Jacobi passes at 128, 256 and 512 threads per block and at 256 as a
+ * resident grid walking the scene tiles (each scene's sorted range cut into
+ * blocks, from the cell table), and the neighbour sweep with 4, 8 and 16
+ * particles per pass, time them (each trial frame synchronises its stream, so
+ * do not capture them in a graph), and keep the fastest shapes for the
+ * context.  The shapes change no result.  pk_ctx_tuning reports the shapes in
+ * use and whether trials remain; pk_ctx_tuning_resident whether the passes
+ * run as the resident grid. */
 int pk_ctx_autotune(pk_ctx* ctx, int enable);
 int pk_ctx_tuning(const pk_ctx* ctx, int* pass_block, int* build_particles, int* active);
+int pk_ctx_tuning_resident(const pk_ctx* ctx, int* resident);
 
 /* Per-kernel timing with CUDA events recorded on the launching stream around
  * each kernel class of the neighbour build and the solver (no reference

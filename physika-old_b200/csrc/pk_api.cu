@@ -55,7 +55,8 @@ int ensure_particles(pk_ctx* c, int n)
               regrow(c->xs_pre, m) && regrow(c->xs0, m) && regrow(c->xa, m) && regrow(c->xb, m) &&
               regrow(c->vs, m) && regrow(c->vv, m) && regrow(c->rho, m) && regrow(c->rcnt, m) &&
               regrow(c->tau, m) && regrow(c->tau_hint, m) && regrow(c->hcnt, m) && regrow(c->items, m + 1) &&
-              regrow(c->nitems, 1) && regrow(c->ovf, m) && regrow(c->ovf_list, m);
+              regrow(c->nitems, 1) && regrow(c->ovf, m) && regrow(c->ovf_list, m) && regrow(c->tile_cnt, m + 2) &&
+              regrow(c->tile_off, m + 2) && regrow(c->tiles, m + m / 128 + 2);
     if (!ok) {
         c->cap_n = 0;
         return fail(c, PK_ERR_NOMEM, "device allocation of particle scratch failed");
@@ -289,7 +290,8 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->xs_pre, c->xs0, c->xa, c->xb, c->vs, c->vv, c->rho, c->rcnt, c->tau, c->tau_hint, c->pl_y1, c->pl_y2, c->pl_i1, c->pl_yield,
                     c->pl_invF, c->pl_sizes, c->pl_off, c->pl_rest_idx2, c->pl_rest_pos2,
                     c->hcnt, c->items, c->nitems,
-                    c->rows, c->hits, c->hpool, c->rpool, c->ovf, c->ovf_list, c->spill, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
+                    c->rows, c->hits, c->hpool, c->rpool, c->ovf, c->ovf_list, c->spill, c->tile_cnt,
+                    c->tile_off, c->tiles, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
                     c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v, c->pd_ktw, c->pl_mk};
@@ -343,7 +345,8 @@ PK_API int pk_ctx_autotune(pk_ctx* c, int enable)
     if (!c) return PK_ERR_ARG;
     cudaSetDevice(c->device);
     auto& t = c->tune;
-    t = pk_ctx::Tune{t.on, 0, t.pass_block, t.build_pb, {0, 0, 0}, {0, 0, 0}, {t.ev[0], t.ev[1], t.ev[2], t.ev[3]}};
+    t = pk_ctx::Tune{t.on, 0, t.pass_block, t.persist, t.build_pb, {0, 0, 0, 0}, {0, 0, 0},
+                     {t.ev[0], t.ev[1], t.ev[2], t.ev[3]}};
     if (!enable) {
         t.on = false;
         return PK_OK;
@@ -361,6 +364,13 @@ PK_API int pk_ctx_tuning(const pk_ctx* c, int* pass_block, int* build_particles,
     if (pass_block) *pass_block = c->tune.pass_block;
     if (build_particles) *build_particles = c->tune.build_pb;
     if (active) *active = c->tune.on ? 1 : 0;
+    return PK_OK;
+}
+
+PK_API int pk_ctx_tuning_resident(const pk_ctx* c, int* resident)
+{
+    if (!c || !resident) return PK_ERR_ARG;
+    *resident = c->tune.persist ? 1 : 0;
     return PK_OK;
 }
 
@@ -754,19 +764,21 @@ void tune_record(pk_ctx* c, int trial)
         cudaGetLastError();
         t.on = false;
         t.pass_block = 256;
+        t.persist = false;
         t.build_pb = 8;
         return;
     }
-    const int pi = t.pass_block == 128 ? 0 : (t.pass_block == 512 ? 2 : 1);
+    const int pi = t.persist ? 3 : (t.pass_block == 128 ? 0 : (t.pass_block == 512 ? 2 : 1));
     const int bi = t.build_pb == 8 ? 1 : (t.build_pb == 4 ? 2 : 0);
     if (t.pass_ms[pi] == 0.f || solve < t.pass_ms[pi]) t.pass_ms[pi] = solve;
     if (t.build_ms[bi] == 0.f || build < t.build_ms[bi]) t.build_ms[bi] = build;
     t.frame = trial + 1;
     if (t.frame < 4) return;
     int best = 1;
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 4; ++k)
         if (t.pass_ms[k] < t.pass_ms[best]) best = k;
     t.pass_block = best == 0 ? 128 : (best == 2 ? 512 : 256);
+    t.persist = best == 3;
     int bb = 0;
     for (int k = 1; k < 3; ++k)
         if (t.build_ms[k] < t.build_ms[bb]) bb = k;
@@ -802,11 +814,13 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     pk::SdfView sv{};
     if (p->boundary) sv = pk::sdf_view(c);
     // autotuning: this frame's trial shapes (4 frames: pass blocks 128, 256,
-    // 512 and build passes of 4, 8 and 16 particles)
+    // 512 and 256 as a resident grid walking scene tiles; build passes of 4,
+    // 8 and 16 particles)
     static const int kTrialPass[4] = {128, 256, 512, 256}, kTrialBuild[4] = {16, 8, 4, 16};
     const int trial = c->tune.on ? c->tune.frame : -1;
     if (trial >= 0) {
         c->tune.pass_block = kTrialPass[trial];
+        c->tune.persist = trial == 3;
         c->tune.build_pb = kTrialBuild[trial];
     }
     // The build state is recorded before anything is launched: the solver

@@ -52,6 +52,9 @@ struct pk_ctx {
     long long pool_need = 0;  // entries the last synchronised build asked for
     uint2* hpool = nullptr;
     int* rpool = nullptr;
+    int* tile_cnt = nullptr;  // persistent passes: tiles per scene (n + 2)
+    int* tile_off = nullptr;  // their exclusive scan (n + 2; [nscenes + 1] = tiles)
+    int2* tiles = nullptr;    // sorted ranges of the tiles (n + n/128 + 2)
     int* ovf = nullptr;       // per sorted particle (valid where its count > row_cap)
     int* ovf_list = nullptr;  // sorted particles with a spill segment
     unsigned long long* spill = nullptr;  // 2 device counters
@@ -140,8 +143,9 @@ struct pk_ctx {
         bool on = false;
         int frame = 0;
         int pass_block = 256;   // Jacobi pass threads per block: 128, 256, 512
+        bool persist = false;   // Jacobi passes as a resident grid walking scene tiles
         int build_pb = 8;       // k_build particles per pass: 4, 8 or 16 (8 measured fastest at 2M)
-        float pass_ms[3] = {0, 0, 0};
+        float pass_ms[4] = {0, 0, 0, 0};  // 128, 256, 512, 256 resident
         float build_ms[3] = {0, 0, 0};
         cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // build start/end, solve start/end
     } tune;

@@ -15,6 +15,8 @@
 // entry and its gathers at one entry index touch a few neighbour cells.
 // Jacobi: pass A reads x, writes (x, lambda) to xl; pass B reads xl only and
 // writes x'.
+#include <algorithm>
+
 #include "pk_kernels.cuh"
 
 namespace pk {
@@ -163,6 +165,7 @@ __global__ void __launch_bounds__(kPassBlock)
 #define PK_PASS_PF 2
 #endif
 constexpr int kPassPrefetch = PK_PASS_PF;
+
 #ifndef PK_PASS_WARPS
 #define PK_PASS_WARPS 0  // resident warps per SM asked of the register allocator (0: none)
 #endif
@@ -223,14 +226,11 @@ __device__ __forceinline__ void dens_one(const float4& a, const float4& xi, cons
     s.sg.x = fmaf(w, w, s.sg.x);
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
-    k_pass_density2(const float4* __restrict__ xs, const int* __restrict__ rows,
-                    const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
-                    float4* __restrict__ xl, float* __restrict__ rho_out, Tail tl)
+__device__ __forceinline__ void density2_particle(int s, const float4* __restrict__ xs,
+                                                  const int* __restrict__ rows, const int2* __restrict__ rcnt,
+                                                  int row_cap, const PassK& k_, float4* __restrict__ xl,
+                                                  float* __restrict__ rho_out, const Tail& tl)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
     const float4 xi = xs[s];
     const int na_all = rcnt[s].x, na = min(na_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
@@ -265,6 +265,41 @@ __global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
     if (rho_out != nullptr) rho_out[s] = rho;
 }
 
+// Tiles of the persistent passes: each scene's sorted range (and the range of
+// the particles outside every grid) cut into tiles of one block's threads, so
+// no tile holds two scenes.  Null tiles: one scene, tile t = [t B, (t+1) B).
+struct SceneTiles {
+    const int2* tile;
+    const int* count;  // device: number of tiles
+};
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
+    k_pass_density2(const float4* __restrict__ xs, const int* __restrict__ rows,
+                    const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
+                    float4* __restrict__ xl, float* __restrict__ rho_out, Tail tl)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) density2_particle(s, xs, rows, rcnt, row_cap, k_, xl, rho_out, tl);
+}
+
+// Persistent form: a grid of resident blocks walks the scene tiles.
+// (32 resident warps per SM asked of the register allocator: the tile loop
+// would otherwise take the kernel past 64 registers and a quarter of them)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
+    k_pass_density2_t(const float4* __restrict__ xs, const int* __restrict__ rows,
+                      const int2* __restrict__ rcnt, int row_cap, int n, PassK k_,
+                      float4* __restrict__ xl, float* __restrict__ rho_out, Tail tl, SceneTiles T)
+{
+    const int nt = T.tile ? *T.count : (n + BLOCK - 1) / BLOCK;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 r = T.tile ? T.tile[t] : make_int2(t * BLOCK, min((t + 1) * BLOCK, n));
+        const int s = r.x + (int)threadIdx.x;
+        if (s < r.y) density2_particle(s, xs, rows, rcnt, row_cap, k_, xl, rho_out, tl);
+    }
+}
+
 struct DispAcc {
     float2 ax, ay, az;
 };
@@ -297,13 +332,10 @@ __device__ __forceinline__ void disp_one(const float4& a, int v, const float4& x
     s.az.x = fmaf(c, dz, s.az.x);
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
-    k_pass_disp2(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
-                 int row_cap, int n, PassK k_, float4* __restrict__ xs_out, Tail tl)
+__device__ __forceinline__ void disp2_particle(int s, const float4* __restrict__ xl, const int* __restrict__ rows,
+                                               const int2* __restrict__ rcnt, int row_cap, const PassK& k_,
+                                               float4* __restrict__ xs_out, const Tail& tl)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
     const float4 xi = xl[s];
     const int nu_all = rcnt[s].y, nu = min(nu_all, row_cap);
     const int4* rq = reinterpret_cast<const int4*>(rows + row_slot(s, 0, row_cap));
@@ -335,6 +367,53 @@ __global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
     }
     // the sums hold -(displacement): d was x_j - x_i
     xs_out[s] = make_float4(xi.x - (a.ax.x + a.ax.y), xi.y - (a.ay.x + a.ay.y), xi.z - (a.az.x + a.az.y), 0.f);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, pass_min_blocks<BLOCK>())
+    k_pass_disp2(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
+                 int row_cap, int n, PassK k_, float4* __restrict__ xs_out, Tail tl)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) disp2_particle(s, xl, rows, rcnt, row_cap, k_, xs_out, tl);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
+    k_pass_disp2_t(const float4* __restrict__ xl, const int* __restrict__ rows, const int2* __restrict__ rcnt,
+                   int row_cap, int n, PassK k_, float4* __restrict__ xs_out, Tail tl, SceneTiles T)
+{
+    const int nt = T.tile ? *T.count : (n + BLOCK - 1) / BLOCK;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 r = T.tile ? T.tile[t] : make_int2(t * BLOCK, min((t + 1) * BLOCK, n));
+        const int s = r.x + (int)threadIdx.x;
+        if (s < r.y) disp2_particle(s, xl, rows, rcnt, row_cap, k_, xs_out, tl);
+    }
+}
+
+// Scene tiles from the cell table: scene s holds the sorted range
+// [start[s K], start[(s+1) K]) (K keys per scene), the particles outside
+// every grid [start[nkeys], n).  One thread per scene.
+__global__ void __launch_bounds__(256) k_tile_count(const int* __restrict__ start, long long scene_keys,
+                                                    int nscenes, long long nkeys, int tile, int* __restrict__ cnt)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > nscenes) return;
+    const int b = q < nscenes ? start[(long long)q * scene_keys] : start[nkeys];
+    const int e = q < nscenes ? start[(long long)(q + 1) * scene_keys] : start[nkeys + 1];
+    cnt[q] = (e - b + tile - 1) / tile;
+}
+
+__global__ void __launch_bounds__(256) k_tile_fill(const int* __restrict__ start, long long scene_keys,
+                                                   int nscenes, long long nkeys, int tile,
+                                                   const int* __restrict__ off, int2* __restrict__ tiles)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > nscenes) return;
+    const int b = q < nscenes ? start[(long long)q * scene_keys] : start[nkeys];
+    const int e = q < nscenes ? start[(long long)(q + 1) * scene_keys] : start[nkeys + 1];
+    int o = off[q];
+    for (int a = b; a < e; a += tile) tiles[o++] = make_int2(a, min(a + tile, e));
 }
 
 // Sorted -> caller order: x, v += (x - x_old)/dt (DP_UpdateVelocity,
@@ -494,6 +573,34 @@ struct LaunchDisp {
         k_pass_disp2<B><<<nb, B, 0, st>>>(xl, rows, rcnt, row_cap, n, pk, out, tl);
     }
 };
+// Resident blocks per SM of a persistent pass kernel (one query per shape).
+template <class K>
+static int resident_blocks(K kernel, int block)
+{
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+    return std::max(1, per_sm) * std::max(1, sms);
+}
+template <int B>
+struct LaunchDensityT {
+    static void run(unsigned, cudaStream_t st, const float4* cur, const int* rows, const int2* rcnt, int row_cap,
+                    int n, PassK pk, float4* xl, float* rho, Tail tl, SceneTiles T)
+    {
+        static const int grid = resident_blocks(k_pass_density2_t<B>, B);
+        k_pass_density2_t<B><<<grid, B, 0, st>>>(cur, rows, rcnt, row_cap, n, pk, xl, rho, tl, T);
+    }
+};
+template <int B>
+struct LaunchDispT {
+    static void run(unsigned, cudaStream_t st, const float4* xl, const int* rows, const int2* rcnt, int row_cap,
+                    int n, PassK pk, float4* out, Tail tl, SceneTiles T)
+    {
+        static const int grid = resident_blocks(k_pass_disp2_t<B>, B);
+        k_pass_disp2_t<B><<<grid, B, 0, st>>>(xl, rows, rcnt, row_cap, n, pk, out, tl, T);
+    }
+};
 template <int B>
 struct LaunchVisc {
     static void run(unsigned nb, cudaStream_t st, const float4* xs, const float4* vin, const float4* vold,
@@ -514,12 +621,29 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
     const float4* cur = c->xs0;
     const PassK pk = pass_k(k, mass);
     const Tail tl{c->rpool, c->ovf};
+    // resident-grid passes (an autotuner shape): scene tiles of batched frames
+    // from the cell table
+    const bool persist = PK_PASS_F32X2 && c->tune.persist;
+    SceneTiles T{nullptr, nullptr};
+    if (persist && c->grid.nscenes > 1) {
+        const int ns = c->grid.nscenes;
+        const unsigned nb = (unsigned)((ns + 1 + 255) / 256);
+        k_tile_count<<<nb, 256, 0, st>>>(c->cell_start, c->grid.scene_keys, ns, c->grid.nkeys, pb, c->tile_cnt);
+        exclusive_scan(c->tile_cnt, ns + 1, c->tile_off, c->scan_part, st);
+        k_tile_fill<<<nb, 256, 0, st>>>(c->cell_start, c->grid.scene_keys, ns, c->grid.nkeys, pb, c->tile_off,
+                                        c->tiles);
+        T = SceneTiles{c->tiles, c->tile_off + ns + 1};
+        launches += 2 + scan_launches();
+    }
     // pass B reads only xl, so it may overwrite the positions pass A read
     // (except xs0, which the velocity update needs)
     for (int it = 0; it < iterations; ++it) {
         const bool last = it == iterations - 1;
         prof_begin(c, PK_PROF_DENSITY, st);
-        if (PK_PASS_F32X2)
+        if (persist)
+            by_block<LaunchDensityT>(pb, nbp, st, cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
+                                     last ? c->rho : nullptr, tl, T);
+        else if (PK_PASS_F32X2)
             by_block<LaunchDensity>(pb, nbp, st, cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb,
                                     last ? c->rho : nullptr, tl);
         else
@@ -527,7 +651,9 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
                 cur, c->rows, c->rcnt, c->row_cap, n, pk, c->xb, last ? c->rho : nullptr, tl);
         prof_end(c, PK_PROF_DENSITY, st);
         prof_begin(c, PK_PROF_DISP, st);
-        if (PK_PASS_F32X2)
+        if (persist)
+            by_block<LaunchDispT>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa, tl, T);
+        else if (PK_PASS_F32X2)
             by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, c->xa, tl);
         else
             k_pass_disp<<<(n + kPassBlock - 1) / kPassBlock, kPassBlock, 0, st>>>(c->xb, c->rows, c->rcnt,

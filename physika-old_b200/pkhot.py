@@ -15,7 +15,7 @@ PK_OK, PK_ERR_ARG, PK_ERR_CUDA, PK_ERR_CAPACITY, PK_ERR_STATE, PK_ERR_NOMEM = ra
 
 EXPORTED = [
     "pk_ctx_create", "pk_ctx_destroy", "pk_last_error", "pk_ctx_status", "pk_last_launch_count",
-    "pk_ctx_profile", "pk_ctx_profile_read", "pk_ctx_autotune", "pk_ctx_tuning",
+    "pk_ctx_profile", "pk_ctx_profile_read", "pk_ctx_autotune", "pk_ctx_tuning", "pk_ctx_tuning_resident",
     "pk_nq_build", "pk_nq_row_stats", "pk_summation_density", "pk_pbd_solve", "pk_integrate",
     "pk_advect", "pk_update_velocity", "pk_fixed_points", "pk_plane_constrain", "pk_viscosity",
     "pk_boundary_set_box", "pk_boundary_constrain", "pk_boundary_jitter", "pk_pbf_step",
@@ -109,6 +109,7 @@ def load():
         "pk_pd_get_rest_shape": ([P, P, P, P, P], I),
         "pk_ctx_autotune": ([P, I], I),
         "pk_ctx_tuning": ([P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)], I),
+        "pk_ctx_tuning_resident": ([P, ctypes.POINTER(I)], I),
         "pk_pd_compute_inverse_k": ([P, F, P], I),
         "pk_pd_begin": ([P, P, I, ctypes.POINTER(PdParams), P], I),
         "pk_pd_enforce": ([P, P, I, ctypes.POINTER(PdParams), P], I),
@@ -413,6 +414,12 @@ class Context:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._check(self.L.pk_ctx_tuning(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, bool(c.value)
+
+    def tuning_resident(self):
+        """Whether the Jacobi passes run as a resident grid walking the scene tiles."""
+        r = ctypes.c_int()
+        self._check(self.L.pk_ctx_tuning_resident(self.h, ctypes.byref(r)))
+        return bool(r.value)
 
     # ---- ElasticityModule step by step, ElastoplasticityModule, FractureModule
     def pd_compute_inverse_k(self, horizon):

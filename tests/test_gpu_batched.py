@@ -50,6 +50,38 @@ def test_batched_equals_per_scene(ctx, seed):
         assert np.array_equal(rho.cpu().numpy(), rho_b[lo:hi]), s
 
 
+def test_tuned_batched_frames_equal_per_scene(ctx):
+    # the autotuner's four trial frames, the last with the Jacobi passes as a
+    # resident grid walking the scene tiles; a few particles of one scene lie
+    # outside every grid (their own tile range after all scenes)
+    b = scenes.batched_mix(seed=3, nscenes=9, n_min=100, n_max=3000)
+    x0 = b.x.copy()
+    x0[b.offsets[4]:b.offsets[4] + 5] = 5.0
+    v0 = np.random.default_rng(3).normal(0, 0.05, x0.shape).astype(np.float32)
+    sc0 = b.scenes[0]
+    prm = pkhot.pbf_params(pkhot.nq_params(sc0.radius, sc0.lo, sc0.hi, sc0.cap),
+                           pkhot.pbd_params(sc0.radius, sc0.spacing, sc0.rest_density, sc0.iterations, sc0.dt),
+                           sc0.gravity, boundary=False)
+    tuned = pkhot.Context(0)
+    tuned.autotune(True)
+    xb, vb = t(x0), t(v0)
+    off = t(b.offsets, np.int32)
+    for _ in range(4):
+        tuned.pbf_step_batched(xb, vb, off, prm)
+    tuned.check_status()
+    assert not tuned.tuning()[2]
+    tuned.close()
+    xb, vb = xb.cpu().numpy(), vb.cpu().numpy()
+    for s in range(len(b.scenes)):
+        lo, hi = b.offsets[s], b.offsets[s + 1]
+        xs, vs = t(x0[lo:hi]), t(v0[lo:hi])
+        for _ in range(4):
+            ctx.pbf_step(xs, vs, prm)
+        ctx.check_status()
+        assert np.array_equal(xs.cpu().numpy(), xb[lo:hi]), s
+        assert np.array_equal(vs.cpu().numpy(), vb[lo:hi]), s
+
+
 def test_batched_arguments(ctx):
     x = t(np.zeros((4, 3)))
     sc = scenes.dam_break_small(n_side=2)

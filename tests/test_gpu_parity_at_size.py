@@ -9,7 +9,8 @@
   positions within 1e-4 and velocities within 1e-3 relative (2-norm over all
   particles), and the densities of the final positions within 1e-4.
 - The same lattice away from the walls, 10 frames, against a double run of
-  the same method: positions within 1e-4 relative.
+  the same method, on the CPU and on the GPU (pk_pbd_rollout_f64): positions
+  within 1e-4 relative.
 - Peridynamics bar, 524,288 particles, cap 80, the left end clamped and the
   right end pulled at 0.5 m/s, fracture off: positions within 1e-5 after one
   step and 1e-4 after 10 steps, against the restatement on the same bonds.
@@ -121,6 +122,25 @@ def test_dam_break_2m_float_against_double_run(ctx, threads):
     ctx.check_status()
     err = rel(x.cpu().numpy(), xo)
     print(f"2M dam break, 10 frames: float vs double relative position error {err:.3e}")
+    assert err < 1e-4
+
+
+def test_dam_break_2m_float_against_gpu_double_run(ctx):
+    # the same off-wall lattice: the float fused frames against the double
+    # frames of the same method on the GPU (pk_pbd_rollout_f64)
+    sc = scenes.dam_break_2m(seed=0)
+    x0 = torch.from_numpy((sc.x + np.array([0.5, 0.3, 0.3], np.float32)).astype(np.float32)).cuda()
+    prm = pkhot.pbf_params(pkhot.nq_params(sc.radius, sc.lo, sc.hi, sc.cap),
+                           pkhot.pbd_params(sc.radius, sc.spacing, sc.rest_density, sc.iterations, sc.dt),
+                           sc.gravity, boundary=False)
+    x, v = x0.clone(), torch.zeros_like(x0)
+    for _ in range(10):
+        ctx.pbf_step(x, v, prm)
+    xd, vd = x0.double(), torch.zeros_like(x0, dtype=torch.float64)
+    ctx.pbd_rollout(xd, vd, prm, 10, 0)
+    ctx.check_status()
+    err = float((x.double() - xd).norm() / xd.norm())
+    print(f"2M dam break, 10 frames: float vs GPU double relative position error {err:.3e}")
     assert err < 1e-4
 
 
