@@ -59,6 +59,31 @@ def build_framework(force=False, verbose=True):
     return out
 
 
+def pkbind_path():
+    import sysconfig
+    return os.path.join(HERE, "lib", "_pkbind" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_pkbind(force=False, verbose=True):
+    """The pybind11 layer of the differentiable rollouts (csrc/pk_pybind.cpp)
+    into lib/_pkbind*.so, linked against libpkhot.so (found next to it)."""
+    import sysconfig
+    import pybind11
+    out = pkbind_path()
+    src = os.path.join(HERE, "csrc", "pk_pybind.cpp")
+    deps = [src, os.path.join(ROOT, "include", "pk_hot.h")]
+    if not force and not _newer(out, deps):
+        return out
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden", "-Wall",
+           "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"], src,
+           "-L", os.path.join(HERE, "lib"), "-lpkhot", "-Wl,-rpath,$ORIGIN", "-o", out + ".tmp"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(out + ".tmp", out)
+    return out
+
+
 # The reference checkout: PK_REFERENCE_SRC, else a directory named `reference`
 # beside this repository.  Only the golden-fixture drivers under oracle/_ref
 # need it; a machine without it uses the prebuilt drivers.
@@ -81,4 +106,5 @@ def build_oracle(verbose=True, with_ref=False):
 if __name__ == "__main__":
     build_pkhot(force="--force" in sys.argv)
     build_framework(force="--force" in sys.argv)
+    build_pkbind(force="--force" in sys.argv)
     build_oracle(with_ref=True)

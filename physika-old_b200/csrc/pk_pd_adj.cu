@@ -502,8 +502,19 @@ __global__ void __launch_bounds__(256)
 
 // Per source particle i: Fbar_i over its bonds, the bulk_i gradient, and
 // G_i = dL/dFraw_i / (tw h) (0 when the identity was taken).
+// Resident blocks per SM asked of the register allocator for the two bond
+// walks of the reverse pass.  Uncapped they took 146 and 88 registers (12 and
+// 20 warps per SM, long-scoreboard bound); at 80 and 64 (112 and 32 bytes of
+// stack for spills) the 200-step backward of the 65,536-particle block went
+// 970 -> 832 ms; 96/78 gave 838 ms, 64/64 885 ms.
+#ifndef PK_ADJB_MINB
+#define PK_ADJB_MINB 6
+#endif
+#ifndef PK_ADJC_MINB
+#define PK_ADJC_MINB 8
+#endif
 template <class R, class RX>
-__global__ void __launch_bounds__(kPdBlock)
+__global__ void __launch_bounds__(kPdBlock, PK_ADJB_MINB)
     k_pd_adjB(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ xn, const RX* __restrict__ bulk,
               const RX* __restrict__ Fst, const float* __restrict__ twst, const R* __restrict__ a,
               R* __restrict__ G, double* __restrict__ bulkbar)
@@ -667,7 +678,7 @@ __global__ void __launch_bounds__(kPdBlock)
 // k_pd_adjC_push keeps k's own sum in gown[k] and the partner terms in the
 // bond slots; k_pd_adjC_gather adds the incoming slots.
 template <class R, class RX>
-__global__ void __launch_bounds__(kPdBlock)
+__global__ void __launch_bounds__(kPdBlock, PK_ADJC_MINB)
     k_pd_adjC_push(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ bulk, const R* __restrict__ a,
                    const R* __restrict__ G, R* __restrict__ gown, R* __restrict__ slot)
 {

@@ -14,10 +14,38 @@ pk_pbd_rollout_backward and returns dL/dx0 and dL/dv0.
 
 float32 and float64 tensors are supported (the float64 path is the reference
 for gradient checks).
+
+Both Functions call the library through its pybind11 layer (lib/_pkbind*.so,
+csrc/pk_pybind.cpp), which checks the tensors and passes torch's current
+stream; importing this module fails when that layer is not built.
 """
+import ctypes
+import importlib.util
+import os
 from dataclasses import dataclass
 
 import torch
+
+
+def _load_pkbind():
+    import sysconfig
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
+                        "_pkbind" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is not built (run __graft_entry__.build())")
+    import pkhot
+    pkhot.load()  # libpkhot.so first, so the layer binds the same instance
+    spec = importlib.util.spec_from_file_location("_pkbind", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_pkbind = _load_pkbind()
+
+
+def _handle(pk_ctx):
+    return int(pk_ctx.h.value)
 
 
 @dataclass
@@ -38,20 +66,21 @@ class PdRollout(torch.autograd.Function):
         x = x0.detach().clone().contiguous()
         v = v0.detach().clone().contiguous()
         b = bulk.detach().contiguous()
+        h = _handle(pk_ctx)
         if x.dtype == torch.float32:
-            pk_ctx.pd_set_bulk(b)
-            pk_ctx.pd_rollout(x, v, s.horizon, s.mu, s.lam, s.iterations, s.dt, s.steps, s.checkpoint_every,
-                              s.gravity)
+            _pkbind.pd_set_bulk(h, b)
+            _pkbind.pd_rollout(h, x, v, s.horizon, s.mu, s.lam, s.iterations, s.dt, s.steps, s.checkpoint_every,
+                               tuple(s.gravity))
         else:
-            pk_ctx.pd_rollout(x, v, s.horizon, s.mu, s.lam, s.iterations, s.dt, s.steps, s.checkpoint_every,
-                              s.gravity, bulk64=b)
+            _pkbind.pd_rollout(h, x, v, s.horizon, s.mu, s.lam, s.iterations, s.dt, s.steps, s.checkpoint_every,
+                               tuple(s.gravity), b)
         fctx.pk_ctx = pk_ctx
         fctx.bulk_dtype = bulk.dtype
         return x
 
     @staticmethod
     def backward(fctx, gx_t):
-        gx, gv, gb = fctx.pk_ctx.pd_rollout_backward(gx_t.contiguous())
+        gx, gv, gb = _pkbind.pd_rollout_backward(_handle(fctx.pk_ctx), gx_t.contiguous())
         return gx, gv, gb.to(fctx.bulk_dtype), None, None
 
 
@@ -65,13 +94,13 @@ class PbdRollout(torch.autograd.Function):
     def forward(fctx, x0, v0, pk_ctx, params, steps, checkpoint_every):
         x = x0.detach().clone().contiguous()
         v = v0.detach().clone().contiguous()
-        pk_ctx.pbd_rollout(x, v, params, steps, checkpoint_every)
+        _pkbind.pbd_rollout(_handle(pk_ctx), x, v, ctypes.addressof(params), steps, checkpoint_every)
         fctx.pk_ctx = pk_ctx
         return x, v
 
     @staticmethod
     def backward(fctx, gx_t, gv_t):
-        gx, gv = fctx.pk_ctx.pbd_rollout_backward(gx_t.contiguous(), gv_t.contiguous())
+        gx, gv = _pkbind.pbd_rollout_backward(_handle(fctx.pk_ctx), gx_t.contiguous(), gv_t.contiguous())
         return gx, gv, None, None, None, None
 
 
