@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(128)
     for (int e = L.sub; e < m; e += 8) {
         const long long at = pd_at(index, cap, i, e);
         const float q0 = rpos[3 * at] - ri0, q1 = rpos[3 * at + 1] - ri1, q2 = rpos[3 * at + 2] - ri2;
-        const float r = sqrtf(q0 * q0 + q1 * q1 + q2 * q2);
+        const float r = exact_norm3(q0, q1, q2);  // (rest_j - rest_i).norm(), as compiled by the reference
         if (r > kEpsilon) {
             const float wt = corr_w(r, h), sw = sqrtf(wt);
             const float q[3] = {q0 / h * sw, q1 / h * sw, q2 / h * sw};

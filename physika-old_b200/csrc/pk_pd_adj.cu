@@ -97,15 +97,24 @@ struct PdBonds {
 };
 
 // CorrectedKernel Weight and WeightRR (Kernel.h:99-142) with q = r * (1/h).
+// The bond geometry every forward and reverse kernel evaluates -- the rest
+// length r and these weights -- is written with every rounding explicit, so
+// each kernel gets the same bits whatever the compiler's contraction choices
+// at its call site: the reverse pass must see the forward's r (a one-ulp
+// difference in r between the forward's F and the reverse's recomputation
+// moved the double adjoint of a 2,000-iteration rollout by 1.4e-4).  r is
+// the reference's compiled Vector3f::norm (exact_norm3).
+__device__ __forceinline__ float bond_len(float e0, float e1, float e2) { return exact_norm3(e0, e1, e2); }
 __device__ __forceinline__ float corr_w_f(float r, float inv_h)
 {
-    const float q = r * inv_h;
-    return q > 1.0f ? 0.0f : q * q * q * (1.0f - q * q);
+    const float q = __fmul_rn(r, inv_h);
+    const float qq = __fmul_rn(q, q);
+    return q > 1.0f ? 0.0f : __fmul_rn(__fmul_rn(qq, q), __fsub_rn(1.0f, qq));
 }
 __device__ __forceinline__ float corr_wrr_f(float r, float inv_h)
 {
-    const float q = r * inv_h;
-    return q > 1.0f ? 0.0f : q * (1.0f - q * q) * (inv_h * inv_h);
+    const float q = __fmul_rn(r, inv_h);
+    return q > 1.0f ? 0.0f : __fmul_rn(__fmul_rn(q, __fsub_rn(1.0f, __fmul_rn(q, q))), __fmul_rn(inv_h, inv_h));
 }
 
 // unit_or_zero without the length: one reciprocal square root.
@@ -121,6 +130,35 @@ __device__ __forceinline__ void unit_fast(V3<R>& u)
     } else {
         u.x = u.y = u.z = (R)0;
     }
+}
+
+// A bond slot holds 4 values (the bond's term and a zero pad) and is written
+// whole in one store: a slot written in part leaves its 32-byte sector
+// partly written, which the L2 completes by reading it from DRAM (k_pd_FP
+// read 1.38 GB per launch on the 524,288-particle bar, half of it that).
+__device__ __forceinline__ void store_slot(float* o, float x, float y, float z)
+{
+    *reinterpret_cast<float4*>(o) = make_float4(x, y, z, 0.f);
+}
+__device__ __forceinline__ void store_slot(double* o, double x, double y, double z)
+{
+    reinterpret_cast<double2*>(o)[0] = make_double2(x, y);
+    reinterpret_cast<double2*>(o)[1] = make_double2(z, 0.0);
+}
+__device__ __forceinline__ void add_slot(const float* g, float& x, float& y, float& z)
+{
+    const float4 q = __ldg(reinterpret_cast<const float4*>(g));
+    x += q.x;
+    y += q.y;
+    z += q.z;
+}
+__device__ __forceinline__ void add_slot(const double* g, double& x, double& y, double& z)
+{
+    const double2 a = __ldg(reinterpret_cast<const double2*>(g));
+    const double b = __ldg(g + 2);
+    x += a.x;
+    y += a.y;
+    z += b;
 }
 
 // Every particle is handled by a group of kPdG lanes of one warp: lane `sub`
@@ -196,13 +234,13 @@ __device__ void pd_deformation(const PdBonds& B, const RX* x, int i, int sub, R 
         if (e + kPdG < m) load(e + kPdG);
         if (stash && k < kPdStash) stash[k][threadIdx.x] = make_float4(e0, e1, e2, __int_as_float(al ? j : ~j));
         if (!al) continue;
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        const float r = bond_len(e0, e1, e2);
         if (r > kEpsilon) {
             const float wt = corr_w_f(r, B.inv_h);
             const V3<R> xj = ld3r<R>(x, j);
             const R ih = (R)B.inv_h;
             const R p[3] = {(xj.x - ci.x) * ih, (xj.y - ci.y) * ih, (xj.z - ci.z) * ih};
-            const float qs = B.inv_h * wt;
+            const float qs = __fmul_rn(B.inv_h, wt);
             const R q[3] = {(R)(e0 * qs), (R)(e1 * qs), (R)(e2 * qs)};
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) F[a][b] += p[a] * q[b];
@@ -274,7 +312,7 @@ __global__ void __launch_bounds__(kPdBlock) k_pd_W(PdBonds B, const RB* __restri
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        const float r = bond_len(e0, e1, e2);
         if (!(r > 0.01f * B.h)) continue;
         w += ml * (R)bulk[i] * (R)corr_wrr_f(r, B.inv_h);
     }
@@ -285,7 +323,7 @@ __global__ void __launch_bounds__(kPdBlock) k_pd_W(PdBonds B, const RB* __restri
         const long long k0 = pd_at(B.index, B.cap, kb.x, 0);
         const float e0 = B.rpos[3 * k0] - B.rpos[3 * at], e1 = B.rpos[3 * k0 + 1] - B.rpos[3 * at + 1],
                     e2 = B.rpos[3 * k0 + 2] - B.rpos[3 * at + 2];
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        const float r = bond_len(e0, e1, e2);
         if (!(r > 0.01f * B.h)) continue;
         w += ml * (R)bulk[kb.x] * (R)corr_wrr_f(r, B.inv_h);
     }
@@ -311,7 +349,7 @@ __global__ void __launch_bounds__(kPdBlock)
         const long long at = pd_at(B.index, B.cap, i, e);
         if (!B.alive[at]) continue;
         const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        const float r = bond_len(e0, e1, e2);
         if (!(r > 0.01f * B.h)) continue;
         const V3<R> xj = ld3(x, B.ridx[at]);
         V3<R> nf = mat_e(Fi, e0, e1, e2);
@@ -333,7 +371,7 @@ __global__ void __launch_bounds__(kPdBlock)
         const long long k0 = pd_at(B.index, B.cap, k, 0);
         const float e0 = B.rpos[3 * k0] - B.rpos[3 * at], e1 = B.rpos[3 * k0 + 1] - B.rpos[3 * at + 1],
                     e2 = B.rpos[3 * k0 + 2] - B.rpos[3 * at + 2];
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        const float r = bond_len(e0, e1, e2);
         if (!(r > 0.01f * B.h)) continue;
         const V3<R> xk = ld3(x, k);
         V3<R> nf = mat_e(F + 9LL * k, e0, e1, e2);
@@ -416,7 +454,7 @@ __global__ void __launch_bounds__(kPdBlock)
             e1 = ri1 - B.rpos[3 * at + 1];
             e2 = ri2 - B.rpos[3 * at + 2];
         }
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+        const float r = bond_len(e0, e1, e2);
         if (al && r > 0.01f * B.h) {
             const V3<R> xj = ld3(x, j);
             V3<R> nf = V3<R>{Fi[0][0] * e0 + Fi[0][1] * e1 + Fi[0][2] * e2, Fi[1][0] * e0 + Fi[1][1] * e1 + Fi[1][2] * e2,
@@ -433,12 +471,7 @@ __global__ void __launch_bounds__(kPdBlock)
             acc.y += t.y;
             acc.z += t.z;
         }
-        if (L.valid) {
-            R* o = tslot + 4 * at;
-            o[0] = t.x;
-            o[1] = t.y;
-            o[2] = t.z;
-        }
+        if (L.valid) store_slot(tslot + 4 * at, t.x, t.y, t.z);
     }
     acc.x = gsum(acc.x);
     acc.y = gsum(acc.y);
@@ -465,9 +498,7 @@ __global__ void __launch_bounds__(kPdBlock)
     for (; t < t1; t += kPdG) {
         const R* g = tslot + 4 * (long long)slot_n;
         if (t + kPdG < t1) slot_n = B.in_list[t + kPdG].y;
-        in.x += g[0];
-        in.y += g[1];
-        in.z += g[2];
+        add_slot(g, in.x, in.y, in.z);
     }
     in.x = gsum(in.x);
     in.y = gsum(in.y);
@@ -500,209 +531,128 @@ __global__ void __launch_bounds__(256)
     xoldbar[3 * i + 2] += ai.z;
 }
 
-// Per source particle i: Fbar_i over its bonds, the bulk_i gradient, and
-// G_i = dL/dFraw_i / (tw h) (0 when the identity was taken).
-// Resident blocks per SM asked of the register allocator for the two bond
-// walks of the reverse pass.  Uncapped they took 146 and 88 registers (12 and
-// 20 warps per SM, long-scoreboard bound); at 80 and 64 (112 and 32 bytes of
-// stack for spills) the 200-step backward of the 65,536-particle block went
-// 970 -> 832 ms; 96/78 gave 838 ms, 64/64 885 ms.
-#ifndef PK_ADJB_MINB
-#define PK_ADJB_MINB 6
-#endif
-#ifndef PK_ADJC_MINB
-#define PK_ADJC_MINB 8
+// Reverse pass of one projection iteration, per source particle i (8 lanes):
+// the first walk over i's bonds forms F-bar_i (through the normalisation
+// Jacobian of n(F e)) and the stiffness gradient of bulk_i; every lane of the
+// group then forms G_i = dL/dF_raw / (tw h) (0 when the identity was taken);
+// the second walk forms dL/dx.  A bond k->i contributes to dL/dx_i through
+// F_k and the n(x_k - x_i) term, and that contribution is formed by the
+// source k, which holds G_k, x_k, a_k and the bond's rest vector: G_k q +
+// dw a_k - u, u the normalisation adjoint of n(x_k - x_i), the same u as in
+// k's own term.  k keeps its own sum in gown[k] and the partner terms in the
+// bond slots, which k_pd_adjC_gather adds.  The second walk reads the first
+// walk's bonds from shared memory; G never goes through global memory.
+// Two kernels (F-bar/G, then dL/dx) at register caps of 80 and 64 took 799 ms
+// for the 200-step backward of the 65,536-particle block; this one at 124
+// registers (4 blocks per SM, no spills) 694 ms, at 96 711 ms, at 80 742 ms.
+#ifndef PK_ADJBC_MINB
+#define PK_ADJBC_MINB 4
 #endif
 template <class R, class RX>
-__global__ void __launch_bounds__(kPdBlock, PK_ADJB_MINB)
-    k_pd_adjB(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ xn, const RX* __restrict__ bulk,
-              const RX* __restrict__ Fst, const float* __restrict__ twst, const R* __restrict__ a,
-              R* __restrict__ G, double* __restrict__ bulkbar)
+__global__ void __launch_bounds__(kPdBlock, PK_ADJBC_MINB)
+    k_pd_adjBC(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ xn, const RX* __restrict__ bulk,
+               const RX* __restrict__ Fst, const float* __restrict__ twst, const R* __restrict__ a,
+               double* __restrict__ bulkbar, R* __restrict__ gown, R* __restrict__ slot)
 {
+    __shared__ float4 stash[kPdStash][kPdBlock];  // (rest_i - rest_j, j or ~j for a dead bond)
     const PdLane L = pd_lane(B.n);
     const int i = L.i;
-    // the forward's F of this iterate, and its tw (negated: identity taken)
-    R F[3][3];
-    for (int p = 0; p < 3; ++p)
-        for (int q = 0; q < 3; ++q) F[p][q] = (R)Fst[9LL * i + 3 * p + q];
-    const float tws = twst[i];
-    const bool ident = tws < 0.f;
-    const float tw = ident ? -1.0f - tws : tws;
     const long long a0 = pd_at(B.index, B.cap, i, 0);
     const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
-    const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i), yi = ld3r<R>(xn, i);
+    const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i);
     const R bulk_i = (R)bulk[i];
     const int m = pd_size(B.index, B.cap, B.total, B.n, i);
-    R Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    R gb = 0;  // d L / d bulk_i
-    for (int e = L.sub; e < m; e += kPdG) {
-        const long long at = pd_at(B.index, B.cap, i, e);
-        if (!B.alive[at]) continue;
-        const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
-        const float r = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
-        if (!(r > 0.01f * B.h)) continue;
-        const int j = B.ridx[at];
-        const V3<R> xj = ld3r<R>(x, j), aj = ld3(a, j);
-        V3<R> nf{F[0][0] * e0 + F[0][1] * e1 + F[0][2] * e2, F[1][0] * e0 + F[1][1] * e1 + F[1][2] * e2,
-                 F[2][0] * e0 + F[2][1] * e1 + F[2][2] * e2};
-        V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
-        const R lf = unit_or_zero(nf);
-        unit_or_zero(nc);
-        const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
-        const R mu = (R)B.mu * bulk_i * wrr;
-        const V3<R> da{ai.x - aj.x, ai.y - aj.y, ai.z - aj.z};
-        // F path
-        const V3<R> ub = unit_vjp(nf, lf, V3<R>{mu * rr * da.x, mu * rr * da.y, mu * rr * da.z});
-        const R ev[3] = {(R)e0, (R)e1, (R)e2};
-        const R ubv[3] = {ub.x, ub.y, ub.z};
+    R Gi[9];
+    {
+        // the forward's F of this iterate, and its tw (negated: identity taken)
+        R F[3][3];
         for (int p = 0; p < 3; ++p)
-            for (int q = 0; q < 3; ++q) Fb[p][q] += ubv[p] * ev[q];
-        // bulk_i: the bond adds w*(target) to D and w to W at both ends, so
-        // d x'/d w = (target - x')/(1 + W) there, with w = mu (or lambda) bulk_i wrr
-        const V3<R> yj = ld3r<R>(xn, j);
-        const R tmu = dot3(ai, V3<R>{xj.x + rr * nf.x - yi.x, xj.y + rr * nf.y - yi.y, xj.z + rr * nf.z - yi.z}) +
-                      dot3(aj, V3<R>{ci.x - rr * nf.x - yj.x, ci.y - rr * nf.y - yj.y, ci.z - rr * nf.z - yj.z});
-        const R tla = dot3(ai, V3<R>{xj.x + rr * nc.x - yi.x, xj.y + rr * nc.y - yi.y, xj.z + rr * nc.z - yi.z}) +
-                      dot3(aj, V3<R>{ci.x - rr * nc.x - yj.x, ci.y - rr * nc.y - yj.y, ci.z - rr * nc.z - yj.z});
-        gb += wrr * ((R)B.mu * tmu + (R)B.lambda * tla);
-    }
-    for (int p = 0; p < 3; ++p)
-        for (int q = 0; q < 3; ++q) Fb[p][q] = gsum(Fb[p][q]);
-    gb = gsum(gb);
-    if (!L.valid || L.sub != 0) return;
-    bulkbar[i] += (double)gb;
-    R Gi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    if (!ident) {
-        if (tw > kEpsilon) {
-            // F = (Fraw / tw) K  =>  dL/dFraw = Fbar K^T / tw
-            const float* K = B.invK + 9LL * i;
-            const R s = (R)1 / ((R)tw * (R)B.h);
-            for (int p = 0; p < 3; ++p)
-                for (int c = 0; c < 3; ++c)
-                    Gi[p][c] = (Fb[p][0] * (R)K[3 * c] + Fb[p][1] * (R)K[3 * c + 1] + Fb[p][2] * (R)K[3 * c + 2]) * s;
-        } else {
-            const R s = (R)1 / (R)B.h;
-            for (int p = 0; p < 3; ++p)
-                for (int c = 0; c < 3; ++c) Gi[p][c] = Fb[p][c] * s;
-        }
-    }
-    for (int p = 0; p < 3; ++p)
-        for (int c = 0; c < 3; ++c) G[9LL * i + 3 * p + c] = Gi[p][c];
-}
-
-// dL/dx_i for the input x of the iteration.
-template <class R, class RX>
-__global__ void __launch_bounds__(kPdBlock)
-    k_pd_adjC(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ bulk, const R* __restrict__ a,
-              const R* __restrict__ G, R* __restrict__ gout)
-{
-    const PdLane L = pd_lane(B.n);
-    const int i = L.i;
-    const long long a0 = pd_at(B.index, B.cap, i, 0);
-    const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
-    const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i);
-    const R bulk_i = (R)bulk[i];
-    const int m = pd_size(B.index, B.cap, B.total, B.n, i);
-    const R* Gi = G + 9LL * i;
-    const R ml = (R)B.mu + (R)B.lambda;
-    V3<R> out{0, 0, 0};
-    for (int e = L.sub; e < m; e += kPdG) {
-        const long long at = pd_at(B.index, B.cap, i, e);
-        if (!B.alive[at]) continue;
-        const int j = B.ridx[at];
-        const float f0 = B.rpos[3 * at] - ri0, f1 = B.rpos[3 * at + 1] - ri1, f2 = B.rpos[3 * at + 2] - ri2;
-        const float r = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
-        // F_i depends on x_i through -(x_i)/h q_j for every first-loop bond
-        if (r > kEpsilon) {
-            const float wt = corr_w_f(r, B.inv_h);
-            const float qs = B.inv_h * wt;
-            const R q0 = (R)(f0 * qs), q1 = (R)(f1 * qs), q2 = (R)(f2 * qs);
-            out.x -= Gi[0] * q0 + Gi[1] * q1 + Gi[2] * q2;
-            out.y -= Gi[3] * q0 + Gi[4] * q1 + Gi[5] * q2;
-            out.z -= Gi[6] * q0 + Gi[7] * q1 + Gi[8] * q2;
-        }
-        if (!(r > 0.01f * B.h)) continue;
-        const V3<R> xj = ld3r<R>(x, j), aj = ld3(a, j);
-        V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
-        const R lc = unit_or_zero(nc);
-        const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
-        const R la = (R)B.lambda * bulk_i * wrr, dw = ml * bulk_i * wrr;
-        const V3<R> uc = unit_vjp(nc, lc, V3<R>{la * rr * (ai.x - aj.x), la * rr * (ai.y - aj.y), la * rr * (ai.z - aj.z)});
-        out.x += dw * aj.x + uc.x;
-        out.y += dw * aj.y + uc.y;
-        out.z += dw * aj.z + uc.z;
-    }
-    for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
-        const int2 kb = B.in_list[t];
-        const long long at = kb.y;
-        if (!B.alive[at]) continue;
-        const int k = kb.x;
-        const long long k0 = pd_at(B.index, B.cap, k, 0);
-        // x_i enters F_k through (x_i - x_k)/h q with q from rest_i - rest_k
-        const float f0 = B.rpos[3 * at] - B.rpos[3 * k0], f1 = B.rpos[3 * at + 1] - B.rpos[3 * k0 + 1],
-                    f2 = B.rpos[3 * at + 2] - B.rpos[3 * k0 + 2];
-        const float r = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
-        if (r > kEpsilon) {
-            const float wt = corr_w_f(r, B.inv_h);
-            const R* Gk = G + 9LL * k;
-            const float qs = B.inv_h * wt;
-            const R q0 = (R)(f0 * qs), q1 = (R)(f1 * qs), q2 = (R)(f2 * qs);
-            out.x += Gk[0] * q0 + Gk[1] * q1 + Gk[2] * q2;
-            out.y += Gk[3] * q0 + Gk[4] * q1 + Gk[5] * q2;
-            out.z += Gk[6] * q0 + Gk[7] * q1 + Gk[8] * q2;
-        }
-        if (!(r > 0.01f * B.h)) continue;
-        const V3<R> xk = ld3r<R>(x, k), ak = ld3(a, k);
-        V3<R> nc{xk.x - ci.x, xk.y - ci.y, xk.z - ci.z};
-        const R lc = unit_or_zero(nc);
-        const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
-        const R la = (R)B.lambda * (R)bulk[k] * wrr, dw = ml * (R)bulk[k] * wrr;
-        const V3<R> uc = unit_vjp(nc, lc, V3<R>{la * rr * (ak.x - ai.x), la * rr * (ak.y - ai.y), la * rr * (ak.z - ai.z)});
-        out.x += dw * ak.x - uc.x;
-        out.y += dw * ak.y - uc.y;
-        out.z += dw * ak.z - uc.z;
-    }
-    out.x = gsum(out.x);
-    out.y = gsum(out.y);
-    out.z = gsum(out.z);
-    if (!L.valid || L.sub != 0) return;
-    gout[3 * i] = out.x;
-    gout[3 * i + 1] = out.y;
-    gout[3 * i + 2] = out.z;
-}
-
-// k_pd_adjC with each bond evaluated once.  The contribution of bond k->i to
-// dL/dx_i (the incoming loop above) is formed by the source k, which holds
-// G_k, x_k, a_k and the bond's rest vector: G_k q + dw a_k - u, u the
-// normalisation adjoint of n(x_k - x_i), the same u as in k's own term.
-// k_pd_adjC_push keeps k's own sum in gown[k] and the partner terms in the
-// bond slots; k_pd_adjC_gather adds the incoming slots.
-template <class R, class RX>
-__global__ void __launch_bounds__(kPdBlock, PK_ADJC_MINB)
-    k_pd_adjC_push(PdBonds B, const RX* __restrict__ x, const RX* __restrict__ bulk, const R* __restrict__ a,
-                   const R* __restrict__ G, R* __restrict__ gown, R* __restrict__ slot)
-{
-    const PdLane L = pd_lane(B.n);
-    const int i = L.i;
-    const long long a0 = pd_at(B.index, B.cap, i, 0);
-    const float ri0 = B.rpos[3 * a0], ri1 = B.rpos[3 * a0 + 1], ri2 = B.rpos[3 * a0 + 2];
-    const V3<R> ci = ld3r<R>(x, i), ai = ld3(a, i);
-    const R bulk_i = (R)bulk[i];
-    const int m = pd_size(B.index, B.cap, B.total, B.n, i);
-    const R* Gi = G + 9LL * i;
-    const R ml = (R)B.mu + (R)B.lambda;
-    V3<R> out{0, 0, 0};
-    for (int e = L.sub; e < m; e += kPdG) {
-        const long long at = pd_at(B.index, B.cap, i, e);
-        V3<R> pt{0, 0, 0};  // the term for the bond's target
-        if (B.alive[at]) {
+            for (int q = 0; q < 3; ++q) F[p][q] = (R)Fst[9LL * i + 3 * p + q];
+        const V3<R> yi = ld3r<R>(xn, i);
+        R Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        R gb = 0;  // d L / d bulk_i
+        for (int e = L.sub, k = 0; e < m; e += kPdG, ++k) {
+            const long long at = pd_at(B.index, B.cap, i, e);
+            const bool al = B.alive[at];
             const int j = B.ridx[at];
-            const float f0 = B.rpos[3 * at] - ri0, f1 = B.rpos[3 * at + 1] - ri1, f2 = B.rpos[3 * at + 2] - ri2;
-            const float r = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
+            const float e0 = ri0 - B.rpos[3 * at], e1 = ri1 - B.rpos[3 * at + 1], e2 = ri2 - B.rpos[3 * at + 2];
+            if (k < kPdStash) stash[k][threadIdx.x] = make_float4(e0, e1, e2, __int_as_float(al ? j : ~j));
+            if (!al) continue;
+            const float r = bond_len(e0, e1, e2);
+            if (!(r > 0.01f * B.h)) continue;
+            const V3<R> xj = ld3r<R>(x, j), aj = ld3(a, j);
+            V3<R> nf{F[0][0] * e0 + F[0][1] * e1 + F[0][2] * e2, F[1][0] * e0 + F[1][1] * e1 + F[1][2] * e2,
+                     F[2][0] * e0 + F[2][1] * e1 + F[2][2] * e2};
+            V3<R> nc{ci.x - xj.x, ci.y - xj.y, ci.z - xj.z};
+            const R lf = unit_or_zero(nf);
+            unit_or_zero(nc);
+            const R wrr = (R)corr_wrr_f(r, B.inv_h), rr = (R)r;
+            const R mu = (R)B.mu * bulk_i * wrr;
+            const V3<R> da{ai.x - aj.x, ai.y - aj.y, ai.z - aj.z};
+            const V3<R> ub = unit_vjp(nf, lf, V3<R>{mu * rr * da.x, mu * rr * da.y, mu * rr * da.z});
+            const R ev[3] = {(R)e0, (R)e1, (R)e2};
+            const R ubv[3] = {ub.x, ub.y, ub.z};
+            for (int p = 0; p < 3; ++p)
+                for (int q = 0; q < 3; ++q) Fb[p][q] += ubv[p] * ev[q];
+            const V3<R> yj = ld3r<R>(xn, j);
+            const R tmu = dot3(ai, V3<R>{xj.x + rr * nf.x - yi.x, xj.y + rr * nf.y - yi.y, xj.z + rr * nf.z - yi.z}) +
+                          dot3(aj, V3<R>{ci.x - rr * nf.x - yj.x, ci.y - rr * nf.y - yj.y, ci.z - rr * nf.z - yj.z});
+            const R tla = dot3(ai, V3<R>{xj.x + rr * nc.x - yi.x, xj.y + rr * nc.y - yi.y, xj.z + rr * nc.z - yi.z}) +
+                          dot3(aj, V3<R>{ci.x - rr * nc.x - yj.x, ci.y - rr * nc.y - yj.y, ci.z - rr * nc.z - yj.z});
+            gb += wrr * ((R)B.mu * tmu + (R)B.lambda * tla);
+        }
+        for (int p = 0; p < 3; ++p)
+            for (int q = 0; q < 3; ++q) Fb[p][q] = gsum(Fb[p][q]);
+        gb = gsum(gb);
+        if (L.valid && L.sub == 0) bulkbar[i] += (double)gb;
+        // G = dL/dF_raw / (tw h): F = (F_raw / tw) K, so dL/dF_raw = F-bar K^T / tw
+        const float tws = twst[i];
+        const bool ident = tws < 0.f;
+        const float tw = ident ? -1.0f - tws : tws;
+        for (int q = 0; q < 9; ++q) Gi[q] = 0;
+        if (!ident) {
+            if (tw > kEpsilon) {
+                const float* K = B.invK + 9LL * i;
+                const R sc = (R)1 / ((R)tw * (R)B.h);
+                for (int p = 0; p < 3; ++p)
+                    for (int c = 0; c < 3; ++c)
+                        Gi[3 * p + c] = (Fb[p][0] * (R)K[3 * c] + Fb[p][1] * (R)K[3 * c + 1] + Fb[p][2] * (R)K[3 * c + 2]) * sc;
+            } else {
+                const R sc = (R)1 / (R)B.h;
+                for (int p = 0; p < 3; ++p)
+                    for (int c = 0; c < 3; ++c) Gi[3 * p + c] = Fb[p][c] * sc;
+            }
+        }
+    }
+    const R ml = (R)B.mu + (R)B.lambda;
+    V3<R> out{0, 0, 0};
+    for (int e = L.sub, k = 0; e < m; e += kPdG, ++k) {
+        const long long at = pd_at(B.index, B.cap, i, e);
+        bool al;
+        int j;
+        float f0, f1, f2;  // rest_j - rest_i
+        if (k < kPdStash) {
+            const float4 q = stash[k][threadIdx.x];
+            const int jv = __float_as_int(q.w);
+            al = jv >= 0;
+            j = al ? jv : ~jv;
+            f0 = -q.x;
+            f1 = -q.y;
+            f2 = -q.z;
+        } else {
+            al = B.alive[at];
+            j = B.ridx[at];
+            f0 = B.rpos[3 * at] - ri0;
+            f1 = B.rpos[3 * at + 1] - ri1;
+            f2 = B.rpos[3 * at + 2] - ri2;
+        }
+        V3<R> pt{0, 0, 0};  // the term for the bond's target
+        if (al) {
+            const float r = bond_len(f0, f1, f2);
             // F_i depends on x_i through -(x_i)/h q and on x_j through +(x_j)/h q
             if (r > kEpsilon) {
                 const float wt = corr_w_f(r, B.inv_h);
-                const float qs = B.inv_h * wt;
+                const float qs = __fmul_rn(B.inv_h, wt);
                 const R q0 = (R)(f0 * qs), q1 = (R)(f1 * qs), q2 = (R)(f2 * qs);
                 const V3<R> gq{Gi[0] * q0 + Gi[1] * q1 + Gi[2] * q2, Gi[3] * q0 + Gi[4] * q1 + Gi[5] * q2,
                                Gi[6] * q0 + Gi[7] * q1 + Gi[8] * q2};
@@ -727,12 +677,7 @@ __global__ void __launch_bounds__(kPdBlock, PK_ADJC_MINB)
                 pt.z += dw * ai.z - uc.z;
             }
         }
-        if (L.valid) {
-            R* o = slot + 4 * at;
-            o[0] = pt.x;
-            o[1] = pt.y;
-            o[2] = pt.z;
-        }
+        if (L.valid) store_slot(slot + 4 * at, pt.x, pt.y, pt.z);
     }
     out.x = gsum(out.x);
     out.y = gsum(out.y);
@@ -751,10 +696,7 @@ __global__ void __launch_bounds__(kPdBlock)
     const int i = L.i;
     V3<R> in{0, 0, 0};
     for (int t = B.in_off[i] + L.sub; t < B.in_off[i + 1]; t += kPdG) {
-        const R* g = slot + 4 * (long long)B.in_list[t].y;
-        in.x += g[0];
-        in.y += g[1];
-        in.z += g[2];
+        add_slot(slot + 4 * (long long)B.in_list[t].y, in.x, in.y, in.z);
     }
     in.x = gsum(in.x);
     in.y = gsum(in.y);
@@ -912,7 +854,7 @@ struct PdWork {
     double* gown = nullptr;   // reverse pass: 3 per particle
     double* aslot = nullptr;  // reverse pass: 4 per bond slot
     long long aslot_cap = 0;
-    double *a = nullptr, *G = nullptr, *g = nullptr, *xoldbar = nullptr, *xb = nullptr,
+    double *a = nullptr, *g = nullptr, *xoldbar = nullptr, *xb = nullptr,
            *vb = nullptr, *Wa = nullptr, *bulkbar = nullptr;
     // rollout record
     int steps = 0, every = 0, n = 0;
@@ -957,7 +899,7 @@ static bool work_alloc(PdWork<R>& w, int n)
     bool ok = realloc_n(w.F, 9 * m) && realloc_n(w.W, m) && realloc_n(w.xold, 3 * m) && realloc_n(w.own, 3 * m) &&
               realloc_n(w.gown, 3 * m) &&
               realloc_n(w.xa, 3 * m) && realloc_n(w.vr, 3 * m) && realloc_n(w.bulk, m) &&
-              realloc_n(w.a, 3 * m) && realloc_n(w.G, 9 * m) && realloc_n(w.g, 3 * m) &&
+              realloc_n(w.a, 3 * m) && realloc_n(w.g, 3 * m) &&
               realloc_n(w.xoldbar, 3 * m) && realloc_n(w.xb, 3 * m) && realloc_n(w.vb, 3 * m) &&
               realloc_n(w.Wa, m) && realloc_n(w.bulkbar, m);
     if (!ok) return false;
@@ -969,7 +911,7 @@ template <class R>
 static void work_free(PdWork<R>* w)
 {
     if (!w) return;
-    void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->own, w->tslot, w->gown, w->aslot, w->a, w->G,
+    void* ps[] = {w->F, w->W, w->xold, w->xa, w->vr, w->bulk, w->own, w->tslot, w->gown, w->aslot, w->a,
                   w->g, w->xoldbar,
                   w->xb, w->vb, w->Wa, w->bulkbar, w->ckpt, w->seg, w->segF, w->segT};
     for (void* p : ps)
@@ -1208,15 +1150,13 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
             for (int k = iters - 1; k >= 0; --k) {
                 k_pd_adjA<double><<<nb, 256, 0, st>>>(n, w->g, w->Wa, w->a, w->xoldbar);
                 const long long slot = (long long)(s - s0) * iters + k;
-                k_pd_adjB<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it + 3LL * n * (k + 1), w->bulk,
-                                                             w->segF + 9LL * n * slot, w->segT + 1LL * n * slot,
-                                                             w->a, w->G, w->bulkbar);
-                k_pd_adjC_push<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, w->bulk, w->a, w->G,
-                                                                      w->gown, w->aslot);
+                k_pd_adjBC<double, R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it + 3LL * n * (k + 1), w->bulk,
+                                                              w->segF + 9LL * n * slot, w->segT + 1LL * n * slot,
+                                                              w->a, w->bulkbar, w->gown, w->aslot);
                 k_pd_adjC_gather<double><<<nb128, kPdBlock, 0, st>>>(B, w->gown, w->aslot, w->g);
             }
             k_pd_adj_tail<double><<<nb3, 256, 0, st>>>(m3, w->g, w->xoldbar, (double)dt, w->xb, w->vb);
-            l += 2 + 4 * iters;
+            l += 2 + 3 * iters;
         }
     }
     k_convert<R, double><<<nb3, 256, 0, st>>>(m3, w->xb, gx);
