@@ -813,6 +813,9 @@ def main():
     ap.add_argument("--elastoplastic-only", action="store_true",
                     help="run only the elastoplastic frame (65,536 particles) and print its dict; for "
                          "profiler captures of that frame")
+    ap.add_argument("--pbd-adjoint-only", action="store_true",
+                    help="run only the DensityPBD rollout and its reverse pass (65,536 particles, 200 frames) and "
+                         "print its dict; for profiler captures of the adjoint kernels")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default shapes (256 threads per pass block, 8 particles per sweep pass) "
                          "instead of tuning during warm-up; for profiler captures, whose serialised "
@@ -827,6 +830,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps(measure_pd(0, args.steps, args.warmup, torch.cuda.synchronize)), flush=True)
+        return 0
+    if args.pbd_adjoint_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(measure_pbd_adjoint(0)), flush=True)
         return 0
     if args.elastoplastic_only:
         import torch
