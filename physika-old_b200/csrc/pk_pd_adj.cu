@@ -145,6 +145,32 @@ __device__ __forceinline__ void store_slot(double* o, double x, double y, double
     reinterpret_cast<double2*>(o)[0] = make_double2(x, y);
     reinterpret_cast<double2*>(o)[1] = make_double2(z, 0.0);
 }
+__device__ __forceinline__ void store_slot(float* o, float x, float y, float z, float w)
+{
+    *reinterpret_cast<float4*>(o) = make_float4(x, y, z, w);
+}
+__device__ __forceinline__ void store_slot(double* o, double x, double y, double z, double w)
+{
+    reinterpret_cast<double2*>(o)[0] = make_double2(x, y);
+    reinterpret_cast<double2*>(o)[1] = make_double2(z, w);
+}
+__device__ __forceinline__ void add_slot(const float* g, float& x, float& y, float& z, float& w)
+{
+    const float4 q = __ldg(reinterpret_cast<const float4*>(g));
+    x += q.x;
+    y += q.y;
+    z += q.z;
+    w += q.w;
+}
+__device__ __forceinline__ void add_slot(const double* g, double& x, double& y, double& z, double& w)
+{
+    const double2 a = __ldg(reinterpret_cast<const double2*>(g));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(g) + 1);
+    x += a.x;
+    y += a.y;
+    z += b.x;
+    w += b.y;
+}
 __device__ __forceinline__ void add_slot(const float* g, float& x, float& y, float& z)
 {
     const float4 q = __ldg(reinterpret_cast<const float4*>(g));
@@ -433,9 +459,12 @@ __global__ void __launch_bounds__(kPdBlock)
     const V3<R> ci = ld3(x, i);
     const int m = pd_size(B.index, B.cap, B.total, B.n, i);
     V3<R> acc{0, 0, 0};
+    R accw = 0;  // the particle's own bond weights (W, the target's share is in the slots)
+    const R ml = (R)B.mu + (R)B.lambda;
     for (int e = L.sub, k = 0; e < m; e += kPdG, ++k) {
         const long long at = pd_at(B.index, B.cap, i, e);
         V3<R> t{0, 0, 0};
+        R wb = 0;
         bool al;
         int j;
         float e0, e1, e2;
@@ -470,42 +499,52 @@ __global__ void __launch_bounds__(kPdBlock)
             acc.x += t.x;
             acc.y += t.y;
             acc.z += t.z;
+            wb = ml * bulk[i] * wrr;
+            accw += wb;
         }
-        if (L.valid) store_slot(tslot + 4 * at, t.x, t.y, t.z);
+        if (L.valid) store_slot(tslot + 4 * at, t.x, t.y, t.z, wb);
     }
     acc.x = gsum(acc.x);
     acc.y = gsum(acc.y);
     acc.z = gsum(acc.z);
+    accw = gsum(accw);
     if (L.valid && L.sub == 0) {
-        own[3 * i] = acc.x;
-        own[3 * i + 1] = acc.y;
-        own[3 * i + 2] = acc.z;
+        own[4 * i] = acc.x;
+        own[4 * i + 1] = acc.y;
+        own[4 * i + 2] = acc.z;
+        own[4 * i + 3] = accw;
     }
 }
 
-// xn = (xold + own - sum of the incoming bond terms) / (1 + W), written about x_i.
+// xn = (xold + own - sum of the incoming bond terms) / (1 + W), written about x_i,
+// W = the particle's own bond weights + those of the bonds naming it (each
+// bond's weight, ml bulk_source wrr, rides in its slot's fourth value, so W
+// follows broken bonds and changed stiffness without a pass of its own).
 template <class R>
 __global__ void __launch_bounds__(kPdBlock)
     k_pd_gather(PdBonds B, const R* __restrict__ x, const R* __restrict__ xold, const R* __restrict__ own,
-                const R* __restrict__ tslot, const R* __restrict__ W, R* __restrict__ xn)
+                const R* __restrict__ tslot, R* __restrict__ xn)
 {
     const PdLane L = pd_lane(B.n);
     const int i = L.i;
     V3<R> in{0, 0, 0};
+    R win = 0;
     const int t1 = B.in_off[i + 1];
     int t = B.in_off[i] + L.sub;
     int slot_n = t < t1 ? B.in_list[t].y : 0;  // the next incoming slot, one bond ahead
     for (; t < t1; t += kPdG) {
         const R* g = tslot + 4 * (long long)slot_n;
         if (t + kPdG < t1) slot_n = B.in_list[t + kPdG].y;
-        add_slot(g, in.x, in.y, in.z);
+        add_slot(g, in.x, in.y, in.z, win);
     }
     in.x = gsum(in.x);
     in.y = gsum(in.y);
     in.z = gsum(in.z);
+    win = gsum(win);
     if (!L.valid || L.sub != 0) return;
-    const V3<R> ci = ld3(x, i), oi = ld3(own, i), xo = ld3(xold, i);
-    const R den = (R)1 + W[i];
+    const V3<R> ci = ld3(x, i), xo = ld3(xold, i);
+    const V3<R> oi{own[4LL * i], own[4LL * i + 1], own[4LL * i + 2]};
+    const R den = (R)1 + (own[4LL * i + 3] + win);
     xn[3 * i] = ci.x + ((xo.x - ci.x) + (oi.x - in.x)) / den;
     xn[3 * i + 1] = ci.y + ((xo.y - ci.y) + (oi.y - in.y)) / den;
     xn[3 * i + 2] = ci.z + ((xo.z - ci.z) + (oi.z - in.z)) / den;
@@ -848,7 +887,7 @@ template <class R>
 struct PdWork {
     int cap_n = 0;
     R *F = nullptr, *W = nullptr, *xold = nullptr, *xa = nullptr, *vr = nullptr, *bulk = nullptr;
-    R* own = nullptr;       // 3 per particle: the sum of its outgoing bond terms
+    R* own = nullptr;       // 4 per particle: the sum of its outgoing bond terms and of their weights
     R* tslot = nullptr;     // 4 per bond slot: the bond's term
     long long tslot_cap = 0;
     double* gown = nullptr;   // reverse pass: 3 per particle
@@ -896,7 +935,7 @@ static bool work_alloc(PdWork<R>& w, int n)
 {
     if (n <= w.cap_n) return true;
     const size_t m = (size_t)n;
-    bool ok = realloc_n(w.F, 9 * m) && realloc_n(w.W, m) && realloc_n(w.xold, 3 * m) && realloc_n(w.own, 3 * m) &&
+    bool ok = realloc_n(w.F, 9 * m) && realloc_n(w.W, m) && realloc_n(w.xold, 3 * m) && realloc_n(w.own, 4 * m) &&
               realloc_n(w.gown, 3 * m) &&
               realloc_n(w.xa, 3 * m) && realloc_n(w.vr, 3 * m) && realloc_n(w.bulk, m) &&
               realloc_n(w.a, 3 * m) && realloc_n(w.g, 3 * m) &&
@@ -999,7 +1038,7 @@ static int project(PdWork<R>& w, const PdBonds& B, R* x, const R* bulk, int iter
     R* nxt = w.xa;
     for (int it = 0; it < iterations; ++it) {
         k_pd_FP<R><<<nb128, kPdBlock, 0, st>>>(B, cur, bulk, w.F, nullptr, w.own, w.tslot);
-        k_pd_gather<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.xold, w.own, w.tslot, w.W, nxt);
+        k_pd_gather<R><<<nb128, kPdBlock, 0, st>>>(B, cur, w.xold, w.own, w.tslot, nxt);
         R* t = cur;
         cur = nxt;
         nxt = t;
@@ -1015,25 +1054,22 @@ int pd_project_solve(pk_ctx* c, float* x, float* v, int n, float horizon, float 
     PdWork<float>* w = ensure_work<float>(c, n);
     if (!w) return -1;
     const PdBonds B = bonds_of(c, horizon, mu, lambda);
-    k_pd_W<float, float><<<pd_groups_blocks(n), kPdBlock, 0, st>>>(B, c->pd_bulk, w->W);
-    int l = 1 + project<float>(*w, B, x, c->pd_bulk, iterations, st);
+    int l = project<float>(*w, B, x, c->pd_bulk, iterations, st);
     const long long m3 = 3LL * n;
     k_pd_vel<float><<<(unsigned)((m3 + 255) / 256), 256, 0, st>>>(m3, v, x, w->xold, dt);
     return l + 1;
 }
 
 // The projection one step at a time (pk_pd_begin / pk_pd_enforce /
-// pk_pd_update_velocity): x_old and the bond weights are kept in the float
-// workspace between the calls.
-int pd_begin(pk_ctx* c, const float* x, int n, float horizon, float mu, float lambda, cudaStream_t st)
+// pk_pd_update_velocity): x_old is kept in the float workspace between the
+// calls (the bond weights come with every iteration's bond terms).
+int pd_begin(pk_ctx* c, const float* x, int n, float /*horizon*/, float /*mu*/, float /*lambda*/, cudaStream_t st)
 {
     PdWork<float>* w = ensure_work<float>(c, n);
     if (!w) return -1;
     if (n <= 0) return 0;
-    const PdBonds B = bonds_of(c, horizon, mu, lambda);
-    k_pd_W<float, float><<<pd_groups_blocks(n), kPdBlock, 0, st>>>(B, c->pd_bulk, w->W);
     cudaMemcpyAsync(w->xold, x, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st);
-    return 1;
+    return 0;
 }
 
 int pd_enforce(pk_ctx* c, float* x, int n, float horizon, float mu, float lambda, cudaStream_t st)
@@ -1044,7 +1080,7 @@ int pd_enforce(pk_ctx* c, float* x, int n, float horizon, float mu, float lambda
     const PdBonds B = bonds_of(c, horizon, mu, lambda);
     const unsigned nb128 = pd_groups_blocks(n);
     k_pd_FP<float><<<nb128, kPdBlock, 0, st>>>(B, x, c->pd_bulk, w->F, nullptr, w->own, w->tslot);
-    k_pd_gather<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->xold, w->own, w->tslot, w->W, w->xa);
+    k_pd_gather<float><<<nb128, kPdBlock, 0, st>>>(B, x, w->xold, w->own, w->tslot, w->xa);
     cudaMemcpyAsync(x, w->xa, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st);
     return 2;
 }
@@ -1084,8 +1120,7 @@ static int rollout(pk_ctx* c, R* x, R* v, const R* bulk_in, int n, const R g[3],
     for (int a = 0; a < 3; ++a) w->gravity[a] = g[a];
     const unsigned nb = (unsigned)((n + 255) / 256);
     const long long m3 = 3LL * n;
-    k_pd_W<R, R><<<pd_groups_blocks(n), kPdBlock, 0, st>>>(B, w->bulk, w->W);
-    int l = 1;
+    int l = 0;
     for (int s = 0; s < steps; ++s) {
         if (every > 0 && s % every == 0) {
             R* ck = w->ckpt + 6LL * n * (s / every);
@@ -1116,9 +1151,8 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
     k_convert<double, R><<<nb3, 256, 0, st>>>(m3, xbar, w->xb);
     k_convert<double, R><<<nb3, 256, 0, st>>>(m3, vbar, w->vb);
     cudaMemsetAsync(w->bulkbar, 0, sizeof(double) * (size_t)n, st);
-    k_pd_W<R, R><<<nb128, kPdBlock, 0, st>>>(B, w->bulk, w->W);
     k_pd_W<double, R><<<nb128, kPdBlock, 0, st>>>(B, w->bulk, w->Wa);
-    int l = 4;
+    int l = 3;
     const int nseg = (w->steps + w->every - 1) / w->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * w->every, s1 = std::min(w->steps, s0 + w->every);
@@ -1137,7 +1171,7 @@ static int rollout_backward(pk_ctx* c, const R* xbar, const R* vbar, R* gx, R* g
                 R* Fk = w->segF + 9LL * n * slot;
                 k_pd_FP<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, w->bulk, Fk, w->segT + 1LL * n * slot,
                                                        w->own, w->tslot);
-                k_pd_gather<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it, w->own, w->tslot, w->W,
+                k_pd_gather<R><<<nb128, kPdBlock, 0, st>>>(B, it + 3LL * n * k, it, w->own, w->tslot,
                                                            it + 3LL * n * (k + 1));
             }
             k_pd_vel<R><<<nb3, 256, 0, st>>>(m3, vr, it + 3LL * n * iters, it, dt);
