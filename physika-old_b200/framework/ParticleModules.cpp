@@ -112,15 +112,19 @@ void NeighborQuery<TDataType>::query(NeighborList<int>& nbr, DeviceArray<Coord>&
                             (long long)nbr.getElements().size(), nullptr, 0),
                 c, "NeighborQuery::compute");
     } else {
-        // sizes first (the reference reduces the counts on the host too,
-        // NeighborQuery.cu:463), then the elements
+        // one build into the list's current elements (the reference reads the
+        // total back and resizes, NeighborQuery.cu:463-472); only a list that
+        // outgrew them is built again at its new size
         long long total = 0;
-        pkCheck(pk_nq_build(c, F(pos), n, &p, nbr.getIndex().getDataPtr(), nullptr, 0, &total, 0), c,
-                "NeighborQuery::compute");
-        if (nbr.getElements().size() < total) nbr.getElements().resize((int)total);
-        pkCheck(pk_nq_build(c, F(pos), n, &p, nbr.getIndex().getDataPtr(), nbr.getElements().getDataPtr(),
-                            (long long)nbr.getElements().size(), &total, 0),
-                c, "NeighborQuery::compute");
+        const long long have = (long long)nbr.getElements().size();
+        int rc = pk_nq_build(c, F(pos), n, &p, nbr.getIndex().getDataPtr(), have > 0 ? nbr.getElements().getDataPtr() : nullptr,
+                             have, &total, 0);
+        if (rc == PK_ERR_CAPACITY || (rc == PK_OK && have == 0 && total > 0)) {
+            nbr.getElements().resize((int)(total + total / 8));
+            rc = pk_nq_build(c, F(pos), n, &p, nbr.getIndex().getDataPtr(), nbr.getElements().getDataPtr(),
+                             (long long)nbr.getElements().size(), &total, 0);
+        }
+        pkCheck(rc, c, "NeighborQuery::compute");
         nbr.setTotal(total);
     }
     nbr.setProducer(c);

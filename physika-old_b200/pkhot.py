@@ -244,12 +244,26 @@ class Context:
             self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index),
                                            _ptr(elements), n * cap, ctypes.byref(tot), _stream()))
             return index[:n], elements, tot.value
-        # dynamic: size first, then fill (the reference also reads the total back)
-        self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index), None, 0,
-                                       ctypes.byref(tot), _stream()))
+        # dynamic: one build into a buffer sized from the last dynamic total (and an
+        # eighth more); only a list that outgrew it is built again at its size (the
+        # reference also reads the total back and resizes, NeighborQuery.cu:463-472)
+        hint = getattr(self, "_dyn_hint", 0)
+        if hint > 0:
+            elements = torch.empty(hint, dtype=torch.int32, device=x.device)
+            rc = self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index), _ptr(elements), hint,
+                                    ctypes.byref(tot), _stream())
+            if rc == PK_OK:
+                self._dyn_hint = max(hint, tot.value + tot.value // 8)
+                return index[:n], elements[: tot.value], tot.value
+            if rc != PK_ERR_CAPACITY:
+                self._check(rc)
+        else:
+            self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index), None, 0,
+                                           ctypes.byref(tot), _stream()))
         elements = torch.empty(max(tot.value, 1), dtype=torch.int32, device=x.device)
         self._check(self.L.pk_nq_build(self.h, _ptr(x), n, ctypes.byref(p), _ptr(index),
                                        _ptr(elements), tot.value, ctypes.byref(tot), _stream()))
+        self._dyn_hint = tot.value + tot.value // 8
         return index[:n], elements[: tot.value], tot.value
 
     def row_stats(self):
