@@ -294,7 +294,7 @@ PK_API int pk_ctx_destroy(pk_ctx* c)
                     c->tile_off, c->tiles, c->cell_cnt, c->cell_start, c->scan_part, c->g_rho, c->g_lam,
                     c->g_dpos, c->g_xold, c->sdf, c->pd_index, c->pd_rest_idx, c->pd_rest_pos,
                     c->pd_alive, c->pd_invK, c->pd_bulk, c->pd_xold, c->pd_delta, c->pd_w,
-                    c->pd_in_cnt, c->pd_in_off, c->pd_in, c->h_x, c->h_v, c->pd_ktw, c->pl_mk};
+                    c->pd_in_cnt, c->pd_in_off, c->pd_in, c->pd_in_slot, c->h_x, c->h_v, c->pd_ktw, c->pl_mk};
     pk::pd_work_release(c);
     pk::pbd_roll_release(c);
     for (void* p : ptrs)
@@ -1099,7 +1099,8 @@ PK_API int pk_pd_init(pk_ctx* c, const float* x, int n, const int* index, const 
         c->pd_cap_rest = bonds;
     }
     if (bonds > c->pd_cap_bonds) {
-        if (!(regrow(c->pd_alive, (size_t)bonds) && regrow(c->pd_in, (size_t)bonds))) {
+        if (!(regrow(c->pd_alive, (size_t)bonds) && regrow(c->pd_in, (size_t)bonds) &&
+              regrow(c->pd_in_slot, (size_t)bonds))) {
             c->pd_cap_bonds = 0;
             return fail(c, PK_ERR_NOMEM, "device allocation of the bond masks failed");
         }
@@ -1404,7 +1405,8 @@ PK_API int pk_pd_reconstruct_rest_shape(pk_ctx* c, const float* x, int n, const 
     std::swap(c->pd_rest_pos, c->pl_rest_pos2);
     std::swap(c->pd_cap_rest, c->pl_cap_rest2);
     if (new_total > c->pd_cap_bonds) {
-        if (!(regrow(c->pd_alive, (size_t)new_total) && regrow(c->pd_in, (size_t)new_total))) {
+        if (!(regrow(c->pd_alive, (size_t)new_total) && regrow(c->pd_in, (size_t)new_total) &&
+              regrow(c->pd_in_slot, (size_t)new_total))) {
             c->pd_cap_bonds = 0;
             return fail(c, PK_ERR_NOMEM, "device allocation of the bond masks failed");
         }

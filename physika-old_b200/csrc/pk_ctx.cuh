@@ -152,6 +152,7 @@ struct pk_ctx {
     int* pd_in_cnt = nullptr;   // incoming bonds per particle (n + 1)
     int* pd_in_off = nullptr;   // their CSR offsets (n + 1)
     int2* pd_in = nullptr;      // (source particle, bond slot) of every incoming bond
+    int* pd_in_slot = nullptr;  // the bond slots alone, in the same order (the gathers' 4-byte stream)
     // projection workspaces (float, double) and the parameters of the last rollout
     void* pbd_roll = nullptr;   // differentiable DensityPBD rollout (pk_pbd_adj.cu)
     void* pd_work32 = nullptr;
