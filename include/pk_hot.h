@@ -262,7 +262,9 @@ int pk_graph_release(pk_ctx* ctx);
 int pk_last_launch_count(const pk_ctx* ctx);
 
 /* Autotuning of the frame kernels (no reference counterpart).  With enable,
- * the next four pk_pbf_step / pk_pbf_step_batched calls are trial frames: they
+ * the next pk_pbf_step / pk_pbf_step_batched call runs the current shapes
+ * untimed (it takes the one-time costs of a first frame) and the four after it
+ * are trial frames: they
  * run the Jacobi passes at 128, 256 and 512 threads per block and at 256 as a
  * resident grid walking the scene tiles (each scene's sorted range cut into
  * blocks, from the cell table), and the neighbour sweep with 4, 8 and 16

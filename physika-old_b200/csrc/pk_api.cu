@@ -772,8 +772,8 @@ void tune_record(pk_ctx* c, int trial)
     const int bi = t.build_pb == 8 ? 1 : (t.build_pb == 4 ? 2 : 0);
     if (t.pass_ms[pi] == 0.f || solve < t.pass_ms[pi]) t.pass_ms[pi] = solve;
     if (t.build_ms[bi] == 0.f || build < t.build_ms[bi]) t.build_ms[bi] = build;
-    t.frame = trial + 1;
-    if (t.frame < 4) return;
+    t.frame = trial + 2;
+    if (trial < 3) return;
     int best = 1;
     for (int k = 0; k < 4; ++k)
         if (t.pass_ms[k] < t.pass_ms[best]) best = k;
@@ -817,7 +817,10 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     // 512 and 256 as a resident grid walking scene tiles; build passes of 4,
     // 8 and 16 particles)
     static const int kTrialPass[4] = {128, 256, 512, 256}, kTrialBuild[4] = {16, 8, 4, 16};
-    const int trial = c->tune.on ? c->tune.frame : -1;
+    // (the first frame after pk_ctx_autotune runs the current shapes untimed:
+    // it pays the one-time costs, first kernel loads and scratch growth,
+    // that would otherwise land on the first trial)
+    const int trial = c->tune.on ? c->tune.frame - 1 : -1;
     if (trial >= 0) {
         c->tune.pass_block = kTrialPass[trial];
         c->tune.persist = trial == 3;
@@ -845,7 +848,10 @@ int pbf_step_impl(pk_ctx* c, float* x, float* v, int n, const pk_pbf_params* p, 
     c->launches = l;
     if ((rc = check_launch(c, what))) return rc;
     c->nq_valid = true;  // for batched scenes: the union of the scenes' lists
-    if (trial >= 0) tune_record(c, trial);
+    if (trial >= 0)
+        tune_record(c, trial);
+    else if (c->tune.on)
+        c->tune.frame = 1;
     return PK_OK;
 }
 

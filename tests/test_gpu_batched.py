@@ -51,7 +51,7 @@ def test_batched_equals_per_scene(ctx, seed):
 
 
 def test_tuned_batched_frames_equal_per_scene(ctx):
-    # the autotuner's four trial frames, the last with the Jacobi passes as a
+    # the autotuner's warm-up frame and four trial frames, the last with the Jacobi passes as a
     # resident grid walking the scene tiles; a few particles of one scene lie
     # outside every grid (their own tile range after all scenes)
     b = scenes.batched_mix(seed=3, nscenes=9, n_min=100, n_max=3000)
@@ -66,7 +66,7 @@ def test_tuned_batched_frames_equal_per_scene(ctx):
     tuned.autotune(True)
     xb, vb = t(x0), t(v0)
     off = t(b.offsets, np.int32)
-    for _ in range(4):
+    for _ in range(5):
         tuned.pbf_step_batched(xb, vb, off, prm)
     tuned.check_status()
     assert not tuned.tuning()[2]
@@ -75,7 +75,7 @@ def test_tuned_batched_frames_equal_per_scene(ctx):
     for s in range(len(b.scenes)):
         lo, hi = b.offsets[s], b.offsets[s + 1]
         xs, vs = t(x0[lo:hi]), t(v0[lo:hi])
-        for _ in range(4):
+        for _ in range(5):
             ctx.pbf_step(xs, vs, prm)
         ctx.check_status()
         assert np.array_equal(xs.cpu().numpy(), xb[lo:hi]), s
