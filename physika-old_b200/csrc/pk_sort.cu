@@ -116,15 +116,33 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* smem_warp, int& 
     return res;
 }
 
+// A thread's kScanItems consecutive values: two 16-byte loads when the array
+// is 16-byte aligned and the group lies inside it (every group but the last).
+__device__ __forceinline__ void scan_load(const int* __restrict__ in, long long base, long long m, bool vec,
+                                          int (&vals)[kScanItems])
+{
+    if (vec && base + kScanItems <= m) {
+        const int4 u = __ldg(reinterpret_cast<const int4*>(in + base));
+        const int4 w = __ldg(reinterpret_cast<const int4*>(in + base) + 1);
+        vals[0] = u.x; vals[1] = u.y; vals[2] = u.z; vals[3] = u.w;
+        vals[4] = w.x; vals[5] = w.y; vals[6] = w.z; vals[7] = w.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) vals[k] = base + k < m ? in[base + k] : 0;
+    }
+}
+static_assert(kScanItems == 8, "two 16-byte loads per thread");
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restrict__ in, long long m,
-                                                              int* __restrict__ part)
+                                                              int* __restrict__ part, bool vec)
 {
     __shared__ int sw[33];
     long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int vals[kScanItems];
+    scan_load(in, base, m, vec, vals);
     int s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k)
-        if (base + k < m) s += in[base + k];
+    for (int k = 0; k < kScanItems; ++k) s += vals[k];
     int tot;
     block_exclusive_scan(s, sw, tot);
     if (threadIdx.x == 0) part[blockIdx.x] = tot;
@@ -146,23 +164,32 @@ __global__ void __launch_bounds__(1024) k_scan_parts(int* __restrict__ part, int
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_down(const int* __restrict__ in, long long m,
                                                             const int* __restrict__ part,
-                                                            int* __restrict__ out)
+                                                            int* __restrict__ out, bool vec)
 {
     __shared__ int sw[33];
     long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     int vals[kScanItems];
+    scan_load(in, base, m, vec, vals);
     int s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        vals[k] = base + k < m ? in[base + k] : 0;
-        s += vals[k];
-    }
+    for (int k = 0; k < kScanItems; ++k) s += vals[k];
     int tot;
     int ex = block_exclusive_scan(s, sw, tot) + part[blockIdx.x];
+    if (vec && base + kScanItems <= m) {
+        int o[kScanItems];
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < m) out[base + k] = ex;
-        ex += vals[k];
+        for (int k = 0; k < kScanItems; ++k) {
+            o[k] = ex;
+            ex += vals[k];
+        }
+        reinterpret_cast<int4*>(out + base)[0] = make_int4(o[0], o[1], o[2], o[3]);
+        reinterpret_cast<int4*>(out + base)[1] = make_int4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            if (base + k < m) out[base + k] = ex;
+            ex += vals[k];
+        }
     }
     if (base < m && base + kScanItems >= m) out[m] = ex;  // the thread holding the last item
 }
@@ -173,9 +200,10 @@ void exclusive_scan(const int* in, long long m, int* out, int* part, cudaStream_
 {
     long long nparts = (m + kScanTile - 1) / kScanTile;
     if (nparts < 1) nparts = 1;
-    k_scan_reduce<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part);
+    const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+    k_scan_reduce<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, vec);
     k_scan_parts<<<1, 1024, 0, st>>>(part, (int)nparts);
-    k_scan_down<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, out);
+    k_scan_down<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, out, vec);
 }
 
 long long scan_parts_needed(long long m) { return (m + kScanTile - 1) / kScanTile + 1; }
@@ -191,37 +219,77 @@ __global__ void __launch_bounds__(256) k_scatter(const int* __restrict__ key, co
     perm[start[key[i]] + rank[i]] = i;
 }
 
-// Sorts the ids of each cell ascending (insertion sort; cells hold ~10-30)
-// and appends the list-build work items: one (begin, end) sorted range per
-// occupied cell, and one item per particle of the last bucket (outside the
-// grid: each queries its own, out-of-range cell).  Buckets above 2048
-// entries (only the outside bucket can be that large) keep their atomic order.
+// Ascending sort of the m <= N ids at p (N a power of two) in registers: a
+// bitonic network over N values padded with INT_MAX, every index fixed at
+// compile time, so no step waits on a memory access.
+template <int N>
+__device__ __forceinline__ void sort_ids(int* __restrict__ p, int m)
+{
+    int v[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = k < m ? p[k] : 0x7fffffff;
+#pragma unroll
+    for (int size = 2; size <= N; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int l = k ^ stride;
+                if (l > k) {
+                    const int lo = min(v[k], v[l]), hi = max(v[k], v[l]);
+                    const bool up = (k & size) == 0;
+                    v[k] = up ? lo : hi;
+                    v[l] = up ? hi : lo;
+                }
+            }
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        if (k < m) p[k] = v[k];
+}
+
+// Sorts the ids of each cell ascending (cells hold ~10-30: a register
+// network for up to 32, insertion sort above) and appends the list-build work
+// items: one (begin, end) sorted range per occupied cell, a warp's cells with
+// one atomic, and one item per particle of the last bucket (outside the grid:
+// each queries its own, out-of-range cell).  Buckets above 2048 entries (only
+// the outside bucket can be that large) keep their atomic order.
 __global__ void __launch_bounds__(256) k_fix_cells(const int* __restrict__ start, long long ncells,
                                                    int* __restrict__ perm, int2* __restrict__ items,
                                                    int* __restrict__ nitems)
 {
-    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncells) return;
-    int a = start[c], b = start[c + 1];
-    int m = b - a;
-    if (m > 0) {
-        if (c < ncells - 1) {
-            items[atomicAdd(nitems, 1)] = make_int2(a, b);
-        } else {
-            int base = atomicAdd(nitems, m);
-            for (int u = 0; u < m; ++u) items[base + u] = make_int2(a + u, a + u + 1);
-        }
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int a = 0, m = 0;
+    if (c < ncells) {
+        a = start[c];
+        m = start[c + 1] - a;
+    }
+    const bool cell = m > 0 && c < ncells - 1;
+    const unsigned occ = __ballot_sync(0xffffffffu, cell);
+    int base = 0;
+    if (lane == 0 && occ) base = atomicAdd(nitems, __popc(occ));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (cell) items[base + __popc(occ & ((1u << lane) - 1u))] = make_int2(a, a + m);
+    if (m > 0 && c == ncells - 1) {
+        const int b0 = atomicAdd(nitems, m);
+        for (int u = 0; u < m; ++u) items[b0 + u] = make_int2(a + u, a + u + 1);
     }
     if (m < 2 || m > 2048) return;
     int* p = perm + a;
-    for (int u = 1; u < m; ++u) {
-        int t = p[u];
-        int w = u - 1;
-        while (w >= 0 && p[w] > t) {
-            p[w + 1] = p[w];
-            --w;
+    if (m <= 16) {
+        sort_ids<16>(p, m);
+    } else if (m <= 32) {
+        sort_ids<32>(p, m);
+    } else {
+        for (int u = 1; u < m; ++u) {
+            int t = p[u];
+            int w = u - 1;
+            while (w >= 0 && p[w] > t) {
+                p[w + 1] = p[w];
+                --w;
+            }
+            p[w + 1] = t;
         }
-        p[w + 1] = t;
     }
 }
 
