@@ -676,6 +676,8 @@ __global__ void __launch_bounds__(256, PK_EMIT_MINB) k_emit(EmitArgs A)
     }
     const int so = valid ? s : 0;
     const uint2* hrow = A.hits + (long long)so * A.rc;
+    // entry q of the solver row: srow[(q >> 2) * 128 + (q & 3)] (row_slot)
+    int* const srow = A.rows + row_slot(so, 0, A.rc);
     // every lane of the warp iterates to the longest row of the warp's groups
     int cmax = cnt;
 #pragma unroll
@@ -716,7 +718,7 @@ __global__ void __launch_bounds__(256, PK_EMIT_MINB) k_emit(EmitArgs A)
             const unsigned bb = __ballot_sync(kFull, fb && !fa) & gmask;
             if (fa) {
                 const int q = nA + __popc(ba & lt_g);
-                A.rows[row_slot(so, q, A.rc)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
+                srow[(q >> 2) * 128 + (q & 3)] = t | kRowFlagA | (fb ? kRowFlagB : 0);
                 if (pub) {
                     const long long o = pbase + q;
                     if (capped ? (q < A.cap) : (o < A.pub_capacity))
@@ -736,7 +738,10 @@ __global__ void __launch_bounds__(256, PK_EMIT_MINB) k_emit(EmitArgs A)
     }
     __syncwarp();
     if (valid) {
-        for (int e = sub; e < nB; e += kEmitG) A.rows[row_slot(so, nA + e, A.rc)] = s_b[grp][e];
+        for (int e = sub; e < nB; e += kEmitG) {
+            const int q = nA + e;
+            srow[(q >> 2) * 128 + (q & 3)] = s_b[grp][e];
+        }
         if (sub == 0) {
             A.rcnt[s] = make_int2(nA, nA + nB);
             if (A.pub_index != nullptr) A.pub_index[ps] = capped ? min(nA, A.cap) : A.offs[ps];

@@ -417,15 +417,17 @@ __global__ void __launch_bounds__(256) k_tile_fill(const int* __restrict__ start
 }
 
 // Sorted -> caller order: x, v += (x - x_old)/dt (DP_UpdateVelocity,
-// DensityPBD.cu:367-378), outDensity.
+// DensityPBD.cu:367-378), outDensity.  One thread per caller particle i
+// (s = inv[i]): the 16-byte sorted values are gathered, the caller's AoS
+// arrays written contiguously.
 __global__ void __launch_bounds__(256)
     k_finish(const float4* __restrict__ xf, const float4* __restrict__ x0, const float4* __restrict__ vs,
-             const float* __restrict__ rho_s, const int* __restrict__ perm, int n, float dt,
+             const float* __restrict__ rho_s, const int* __restrict__ inv, int n, float dt,
              float* __restrict__ x, float* __restrict__ v, float* __restrict__ rho_out)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    int i = perm[s];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = inv[i];
     float4 p = xf[s], q = x0[s], u = vs[s];
     x[3 * i] = p.x;
     x[3 * i + 1] = p.y;
@@ -508,15 +510,16 @@ __global__ void __launch_bounds__(BLOCK)
                           vo.z / (1.0f + b) + dz_ / t * b / (1.0f + b), 0.f);
 }
 
-// Sorted -> caller order with the velocity given: x, v, outDensity.
+// Sorted -> caller order with the velocity given: x, v, outDensity (one
+// thread per caller particle, as k_finish).
 __global__ void __launch_bounds__(256)
     k_finish_v(const float4* __restrict__ xf, const float4* __restrict__ vf, const float* __restrict__ rho_s,
-               const int* __restrict__ perm, int n, float* __restrict__ x, float* __restrict__ v,
+               const int* __restrict__ inv, int n, float* __restrict__ x, float* __restrict__ v,
                float* __restrict__ rho_out)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const int i = perm[s];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = inv[i];
     const float4 p = xf[s], u = vf[s];
     x[3 * i] = p.x;
     x[3 * i + 1] = p.y;
@@ -677,10 +680,10 @@ int pbd_fast_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iterations,
             vin = vout;
             vout = tmp;
         }
-        k_finish_v<<<nb1, 256, 0, st>>>(cur, vin, c->rho, c->perm, n, x, v, rho);
+        k_finish_v<<<nb1, 256, 0, st>>>(cur, vin, c->rho, c->inv, n, x, v, rho);
         launches += 2 + vis_iterations;
     } else {
-        k_finish<<<nb1, 256, 0, st>>>(cur, c->xs0, c->vs, c->rho, c->perm, n, dt, x, v, rho);
+        k_finish<<<nb1, 256, 0, st>>>(cur, c->xs0, c->vs, c->rho, c->inv, n, dt, x, v, rho);
         ++launches;
     }
     prof_end(c, PK_PROF_FINISH, st);
@@ -707,7 +710,7 @@ int pbd_replay_solve(pk_ctx* c, int n, const Spiky& k, float mass, int iteration
         by_block<LaunchDisp>(pb, nbp, st, c->xb, c->rows, c->rcnt, c->row_cap, n, pk, ys + (size_t)(it + 1) * n,
                              tl);
     }
-    k_finish<<<nb1, 256, 0, st>>>(ys + (size_t)iterations * n, ys, c->vs, c->rho, c->perm, n, dt, x, v, nullptr);
+    k_finish<<<nb1, 256, 0, st>>>(ys + (size_t)iterations * n, ys, c->vs, c->rho, c->inv, n, dt, x, v, nullptr);
     return 2 * iterations + 1;
 }
 
