@@ -121,6 +121,77 @@ class Clocks:
         return out
 
 
+class NvmlClocks:
+    """In-process NVML sampling (read-only queries) of the SM clock, its maximum
+    and the clock-event reasons every 5 ms during a region, so that a region of
+    ~0.1 s still gets samples; falls back to nvidia-smi sampling when NVML is
+    not importable or the device is not found."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
+
+    def __init__(self, bus_id=None):
+        self.bus_id = bus_id
+        self.fallback = None
+        self.samples = []
+        self.thread = None
+        self.running = False
+        self.nv = None
+        self.h = None
+
+    def start(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByPciBusId((self.bus_id + ".0").encode()) if self.bus_id \
+                else nv.nvmlDeviceGetHandleByIndex(0)
+            get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        except Exception:
+            self.nv = None
+            self.fallback = Clocks(self.bus_id)
+            self.fallback.start()
+            return
+
+        def run():
+            while self.running:
+                try:
+                    self.samples.append((float(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)),
+                                         int(get(self.h))))
+                except Exception:
+                    pass
+                time.sleep(0.005)
+
+        self.running = True
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.fallback is not None:
+            return self.fallback.stop()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": "nvml"}
+        if self.nv is None:
+            return out
+        self.running = False
+        self.thread.join(1.0)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.samples:
+            return out
+        reasons = sorted({name for _, bits in self.samples for name, attr, dflt in self.REASONS
+                          if bits & getattr(self.nv, attr, dflt)})
+        out.update(sm_mhz=statistics.median(c for c, _ in self.samples), sm_max_mhz=self.sm_max,
+                   reasons=reasons, samples=len(self.samples))
+        return out
+
+
 def bus_id_of(dev):
     try:
         import torch
@@ -675,7 +746,7 @@ def run_pk(args):
     launches_per_step = ctx.launch_count()
     barrier()
 
-    clocks = Clocks(bus_id_of(local))
+    clocks = NvmlClocks(bus_id_of(local))
     clocks.start()
     ctx.profile(True)
     stream = torch.cuda.current_stream()

@@ -8,6 +8,8 @@
 // round trip), a scatter places ids, and a per-cell fix-up sorts each cell's
 // ids ascending so the order is deterministic.  A final gather builds the
 // sorted float4 arrays the list build and the solver read.
+#include <algorithm>
+
 #include "pk_boundary.cuh"
 #include "pk_kernels.cuh"
 
@@ -162,9 +164,16 @@ __global__ void __launch_bounds__(1024) k_scan_parts(int* __restrict__ part, int
     }
 }
 
+// kItems (the cell table's scan, m = cells + 1 with the last the bucket of
+// particles outside the grid): also appends the list-build work items, one
+// (begin, end) sorted range per occupied cell (a warp's with one atomic) and
+// one per particle of the outside bucket (each queries its own, out-of-range
+// cell).
+template <bool kItems>
 __global__ void __launch_bounds__(kScanThreads) k_scan_down(const int* __restrict__ in, long long m,
                                                             const int* __restrict__ part,
-                                                            int* __restrict__ out, bool vec)
+                                                            int* __restrict__ out, bool vec,
+                                                            int2* __restrict__ items, int* __restrict__ nitems)
 {
     __shared__ int sw[33];
     long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
@@ -175,23 +184,54 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_down(const int* __restric
     for (int k = 0; k < kScanItems; ++k) s += vals[k];
     int tot;
     int ex = block_exclusive_scan(s, sw, tot) + part[blockIdx.x];
-    if (vec && base + kScanItems <= m) {
-        int o[kScanItems];
+    int o[kScanItems];
 #pragma unroll
-        for (int k = 0; k < kScanItems; ++k) {
-            o[k] = ex;
-            ex += vals[k];
-        }
+    for (int k = 0; k < kScanItems; ++k) {
+        o[k] = ex;
+        ex += vals[k];
+    }
+    if (vec && base + kScanItems <= m) {
         reinterpret_cast<int4*>(out + base)[0] = make_int4(o[0], o[1], o[2], o[3]);
         reinterpret_cast<int4*>(out + base)[1] = make_int4(o[4], o[5], o[6], o[7]);
     } else {
 #pragma unroll
-        for (int k = 0; k < kScanItems; ++k) {
-            if (base + k < m) out[base + k] = ex;
-            ex += vals[k];
-        }
+        for (int k = 0; k < kScanItems; ++k)
+            if (base + k < m) out[base + k] = o[k];
     }
     if (base < m && base + kScanItems >= m) out[m] = ex;  // the thread holding the last item
+    if (kItems) {
+        const int lane = threadIdx.x & 31;
+        int occ = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) occ += (base + k < m - 1 && vals[k] > 0) ? 1 : 0;
+        int incl = occ;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        int wbase = 0;
+        if (lane == 31 && incl > 0) wbase = atomicAdd(nitems, incl);
+        wbase = __shfl_sync(0xffffffffu, wbase, 31);
+        int q = wbase + incl - occ;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+            if (base + k < m - 1 && vals[k] > 0) items[q++] = make_int2(o[k], o[k] + vals[k]);
+        if (base <= m - 1 && m - 1 < base + kScanItems) {  // the outside bucket
+            const int k = (int)(m - 1 - base);
+            int cnt = 0, beg = 0;
+#pragma unroll
+            for (int u = 0; u < kScanItems; ++u)
+                if (u == k) {
+                    cnt = vals[u];
+                    beg = o[u];
+                }
+            if (cnt > 0) {
+                const int b0 = atomicAdd(nitems, cnt);
+                for (int u = 0; u < cnt; ++u) items[b0 + u] = make_int2(beg + u, beg + u + 1);
+            }
+        }
+    }
 }
 
 int scan_launches() { return 3; }
@@ -203,7 +243,20 @@ void exclusive_scan(const int* in, long long m, int* out, int* part, cudaStream_
     const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
     k_scan_reduce<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, vec);
     k_scan_parts<<<1, 1024, 0, st>>>(part, (int)nparts);
-    k_scan_down<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, out, vec);
+    k_scan_down<false><<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, out, vec, nullptr, nullptr);
+}
+
+// The cell table's scan (m = cells + 1), appending the list-build items to
+// items / *nitems (zeroed by the caller).
+static void scan_cells(const int* in, long long m, int* out, int* part, int2* items, int* nitems,
+                       cudaStream_t st)
+{
+    long long nparts = (m + kScanTile - 1) / kScanTile;
+    if (nparts < 1) nparts = 1;
+    const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+    k_scan_reduce<<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, vec);
+    k_scan_parts<<<1, 1024, 0, st>>>(part, (int)nparts);
+    k_scan_down<true><<<(unsigned)nparts, kScanThreads, 0, st>>>(in, m, part, out, vec, items, nitems);
 }
 
 long long scan_parts_needed(long long m) { return (m + kScanTile - 1) / kScanTile + 1; }
@@ -247,49 +300,47 @@ __device__ __forceinline__ void sort_ids(int* __restrict__ p, int m)
         if (k < m) p[k] = v[k];
 }
 
-// Sorts the ids of each cell ascending (cells hold ~10-30: a register
-// network for up to 32, insertion sort above) and appends the list-build work
-// items: one (begin, end) sorted range per occupied cell, a warp's cells with
-// one atomic, and one item per particle of the last bucket (outside the grid:
-// each queries its own, out-of-range cell).  Buckets above 2048 entries (only
-// the outside bucket can be that large) keep their atomic order.
-__global__ void __launch_bounds__(256) k_fix_cells(const int* __restrict__ start, long long ncells,
-                                                   int* __restrict__ perm, int2* __restrict__ items,
-                                                   int* __restrict__ nitems)
+// Insertion sort of the m ids at p (cells above 32 ids: dense clusters and
+// the outside bucket).
+__device__ __forceinline__ void sort_ids_insertion(int* __restrict__ p, int m)
 {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    int a = 0, m = 0;
-    if (c < ncells) {
-        a = start[c];
-        m = start[c + 1] - a;
-    }
-    const bool cell = m > 0 && c < ncells - 1;
-    const unsigned occ = __ballot_sync(0xffffffffu, cell);
-    int base = 0;
-    if (lane == 0 && occ) base = atomicAdd(nitems, __popc(occ));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (cell) items[base + __popc(occ & ((1u << lane) - 1u))] = make_int2(a, a + m);
-    if (m > 0 && c == ncells - 1) {
-        const int b0 = atomicAdd(nitems, m);
-        for (int u = 0; u < m; ++u) items[b0 + u] = make_int2(a + u, a + u + 1);
-    }
-    if (m < 2 || m > 2048) return;
-    int* p = perm + a;
-    if (m <= 16) {
-        sort_ids<16>(p, m);
-    } else if (m <= 32) {
-        sort_ids<32>(p, m);
-    } else {
-        for (int u = 1; u < m; ++u) {
-            int t = p[u];
-            int w = u - 1;
-            while (w >= 0 && p[w] > t) {
-                p[w + 1] = p[w];
-                --w;
-            }
-            p[w + 1] = t;
+    for (int u = 1; u < m; ++u) {
+        int t = p[u];
+        int w = u - 1;
+        while (w >= 0 && p[w] > t) {
+            p[w + 1] = p[w];
+            --w;
         }
+        p[w + 1] = t;
+    }
+}
+
+// Sorts the ids of each occupied cell ascending, so the order inside a cell
+// is deterministic (the scatter's order is the atomics' arrival order): one
+// thread per work item (a register network for up to 32 ids, insertion sort
+// above; per-particle items of the outside bucket hold one id), and the
+// outside bucket itself by one thread.  Cells above 2048 ids (only the
+// outside bucket is likely to be that large) keep their arrival order.
+__global__ void __launch_bounds__(256) k_sort_cells(const int* __restrict__ start, long long ncells,
+                                                    int* __restrict__ perm, const int2* __restrict__ items,
+                                                    const int* __restrict__ nitems)
+{
+    const int ni = *nitems;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ni; q += gridDim.x * blockDim.x) {
+        const int2 r = items[q];
+        const int m = r.y - r.x;
+        if (m < 2 || m > 2048) continue;
+        int* p = perm + r.x;
+        if (m <= 16)
+            sort_ids<16>(p, m);
+        else if (m <= 32)
+            sort_ids<32>(p, m);
+        else
+            sort_ids_insertion(p, m);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int a = start[ncells - 1], m = start[ncells] - a;
+        if (m >= 2 && m <= 2048) sort_ids_insertion(perm + a, m);
     }
 }
 
@@ -342,13 +393,12 @@ int sort_particles(pk_ctx* c, float* x, float* v, const float* f, int n, const G
             k_keys<false><<<nb, 256, 0, st>>>(x, v, n, g, c->key, c->rank, c->cell_cnt, sv, nfric, tfric, dt);
         ++launches;
     }
-    exclusive_scan(c->cell_cnt, nk, c->cell_start, c->scan_part, st);
+    cudaMemsetAsync(c->nitems, 0, sizeof(int), st);
+    scan_cells(c->cell_cnt, nk, c->cell_start, c->scan_part, c->items, c->nitems, st);
     launches += scan_launches();
     if (n > 0) {
         k_scatter<<<nb, 256, 0, st>>>(c->key, c->rank, c->cell_start, n, c->perm);
-        cudaMemsetAsync(c->nitems, 0, sizeof(int), st);
-        k_fix_cells<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(c->cell_start, nk, c->perm,
-                                                                   c->items, c->nitems);
+        k_sort_cells<<<std::min(nb, 2048u), 256, 0, st>>>(c->cell_start, nk, c->perm, c->items, c->nitems);
         if (integrate)
             k_gather<true><<<nb, 256, 0, st>>>(x, v, f, c->perm, n, c->xs_pre, c->xs0, c->vs, c->inv,
                                                grav[0], grav[1], grav[2], dt);
